@@ -1,0 +1,167 @@
+/*
+ * qpb.h -- C ABI of libqpb, the batched interior-point QP solver for B200.
+ *
+ * Every entry point solves a batch of independent QPs of one shape
+ *   min 1/2 x'Qx + q'x   s.t.  A x = b,  G x <= h
+ * on the GPU, one persistent launch per call, stream-ordered, without host
+ * synchronisation.  All array arguments are DEVICE pointers to FP64 row-major
+ * data with a leading instance axis (the axis qpax users vmap over):
+ *   Q[batch][n][n], q[batch][n], A[batch][m][n], b[batch][m],
+ *   G[batch][p][n], h[batch][p]; outputs likewise.
+ * Outputs must not alias inputs.  The caller owns every buffer; scratch
+ * comes from `workspace` (size from qpb_workspace_size, 256-byte aligned).
+ * Functions return QPB_OK or a qpb_status code and never abort; a rejected
+ * call launches nothing.  Per-instance convergence is reported in
+ * `converged` / `iters` exactly as qpax returns them.
+ *
+ * Each entry point replaces one function of qpax (kevin-tracy/qpax, v0.0.9);
+ * the citation is on the declaration.  Defaults of the qpax Python API
+ * (solver_tol, target_kappa) live in the Python layer, as in qpax.
+ */
+#ifndef QPB_H_
+#define QPB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct CUstream_st;
+typedef struct CUstream_st* qpb_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum {
+  QPB_OK = 0,
+  QPB_ERR_INVALID_ARGUMENT = 1, /* null / misaligned pointer, negative size, bad option */
+  QPB_ERR_UNSUPPORTED = 2,      /* shape outside the supported range (n, m <= 256), or an
+                                   entry point qpax itself cannot evaluate (p == 0 relax) */
+  QPB_ERR_WORKSPACE = 3,        /* workspace smaller than qpb_workspace_size() */
+  QPB_ERR_CUDA = 4              /* a CUDA runtime call failed (launch, attributes) */
+} qpb_status;
+
+typedef enum { QPB_PRECISION_MIXED = 0, QPB_PRECISION_FP64 = 1 } qpb_precision;
+
+typedef enum {
+  QPB_OP_SOLVE = 0,
+  QPB_OP_INITIALIZE = 1,
+  QPB_OP_RELAX = 2,
+  QPB_OP_PRIMAL_BWD = 3,
+  QPB_OP_DIFF = 4,
+  QPB_OP_ELASTIC_SOLVE = 5,
+  QPB_OP_ELASTIC_INITIALIZE = 6,
+  QPB_OP_ELASTIC_RELAX = 7,
+  QPB_OP_ELASTIC_PRIMAL_BWD = 8,
+  QPB_OP_ELASTIC_DIFF = 9
+} qpb_op;
+
+typedef struct {
+  int32_t batch; /* number of instances (>= 0) */
+  int32_t n;     /* variables (1..256) */
+  int32_t m;     /* equality rows (0..256); 0 for the elastic entry points */
+  int32_t p;     /* inequality rows (>= 0; >= 1 where noted) */
+} qpb_dims;
+
+/* Optional tuning; pass NULL for defaults. */
+typedef struct {
+  int32_t precision;    /* qpb_precision; default QPB_PRECISION_MIXED */
+  int32_t team_threads; /* threads per instance: 0 = automatic, 32, 128 or 256 */
+  double pivot_max;     /* mixed: FP32 factor used while max(d)/min(d) <= pivot_max (0 = 1e5) */
+  int32_t max_sweeps;   /* mixed: FP64 refinement sweeps per solve before FP64 refactor (0 = 8) */
+  int32_t* stats;       /* optional device int32[batch][4]: FP32 factorisations, FP64
+                           factorisations, refinement sweeps, flag bits (1 FP32 factor
+                           rejected, 2 refinement stalled, 4 FP64 pivot breakdown) */
+} qpb_config;
+
+/* Bytes of device workspace an entry point needs for these dims/config. */
+size_t qpb_workspace_size(int32_t op, const qpb_dims* dims, const qpb_config* cfg);
+
+/* qpax/pdip.py:181-251 solve_qp(Q, q, A, b, G, h, solver_tol) ->
+ * (x, s, z, y, converged, iters).  Q is symmetrized, h = +-inf rows are
+ * dropped (s = inf, z = 0 on return), p == 0 takes qpax's direct exits
+ * (converged = 1, iters = 0). s, z may be NULL when p == 0, y when m == 0. */
+int qpb_solve_qp(const qpb_dims* dims, const double* Q, const double* q, const double* A, const double* b,
+                 const double* G, const double* h, double solver_tol, double* x, double* s, double* z, double* y,
+                 int32_t* converged, int32_t* iters, const qpb_config* cfg, void* workspace,
+                 size_t workspace_bytes, qpb_stream_t stream);
+
+/* qpax/pdip.py:15-35 initialize(Q, q, A, b, G, h) -> (x, s, z, y), on the data as given. */
+int qpb_initialize(const qpb_dims* dims, const double* Q, const double* q, const double* A, const double* b,
+                   const double* G, const double* h, double* x, double* s, double* z, double* y,
+                   const qpb_config* cfg, void* workspace, size_t workspace_bytes, qpb_stream_t stream);
+
+/* qpax/pdip_relaxed.py:70-103 relax_qp(Q, q, A, b, G, h, x, s, z, y, solver_tol, target_kappa)
+ * -> (xr, sr, zr, yr, converged, iters).  Requires p >= 1. */
+int qpb_relax_qp(const qpb_dims* dims, const double* Q, const double* q, const double* A, const double* b,
+                 const double* G, const double* h, const double* x_in, const double* s_in, const double* z_in,
+                 const double* y_in, double solver_tol, double target_kappa, double* x, double* s, double* z,
+                 double* y, int32_t* converged, int32_t* iters, const qpb_config* cfg, void* workspace,
+                 size_t workspace_bytes, qpb_stream_t stream);
+
+/* qpax/diff_qp.py:20-46 diff_qp(Q, q, A, b, G, h, x, s, lam, nu, dl_dx)
+ * -> (dQ, dq, dA, db, dG, dh) at a given (relaxed) iterate.  Requires p >= 1. */
+int qpb_diff_qp(const qpb_dims* dims, const double* Q, const double* q, const double* A, const double* b,
+                const double* G, const double* h, const double* x, const double* s, const double* lam,
+                const double* nu, const double* dl_dx, double* dQ, double* dq, double* dA, double* db, double* dG,
+                double* dh, const qpb_config* cfg, void* workspace, size_t workspace_bytes, qpb_stream_t stream);
+
+/* Backward pass of qpax/diff_qp.py:49-82 solve_qp_primal (the custom_vjp):
+ * relax_qp from the forward iterate (x, s, z, y) returned by qpb_solve_qp,
+ * then diff_qp at the relaxed iterate, in one launch.  Only (x, s, z, y) is
+ * kept between forward and backward; the factor is recomputed here.
+ * xr..yr, converged, iters (of the relaxation) may be NULL.  Requires p >= 1. */
+int qpb_solve_qp_primal_bwd(const qpb_dims* dims, const double* Q, const double* q, const double* A,
+                            const double* b, const double* G, const double* h, const double* x, const double* s,
+                            const double* z, const double* y, const double* dl_dx, double solver_tol,
+                            double target_kappa, double* dQ, double* dq, double* dA, double* db, double* dG,
+                            double* dh, double* xr, double* sr, double* zr, double* yr, int32_t* converged,
+                            int32_t* iters, const qpb_config* cfg, void* workspace, size_t workspace_bytes,
+                            qpb_stream_t stream);
+
+/* qpax/elastic_qp.py:184-228 solve_qp_elastic(Q, q, G, h, penalty, solver_tol)
+ * -> (x, t, s1, s2, z1, z2, converged, iters).  dims->m must be 0, p >= 1;
+ * penalty holds one value per instance. */
+int qpb_solve_qp_elastic(const qpb_dims* dims, const double* Q, const double* q, const double* G,
+                         const double* h, const double* penalty, double solver_tol, double* x, double* t,
+                         double* s1, double* s2, double* z1, double* z2, int32_t* converged, int32_t* iters,
+                         const qpb_config* cfg, void* workspace, size_t workspace_bytes, qpb_stream_t stream);
+
+/* qpax/elastic_qp.py:27-47 initialize_elastic -> (x, t, s1, s2, z1, z2). */
+int qpb_initialize_elastic(const qpb_dims* dims, const double* Q, const double* q, const double* G,
+                           const double* h, const double* penalty, double* x, double* t, double* s1, double* s2,
+                           double* z1, double* z2, const qpb_config* cfg, void* workspace, size_t workspace_bytes,
+                           qpb_stream_t stream);
+
+/* qpax/elastic_qp.py:319-359 relax_qp_elastic from (x_in, t_in, s1_in, s2_in, z1_in, z2_in). */
+int qpb_relax_qp_elastic(const qpb_dims* dims, const double* Q, const double* q, const double* G,
+                         const double* h, const double* penalty, const double* const iterate_in[6],
+                         double solver_tol, double target_kappa, double* const iterate_out[6],
+                         int32_t* converged, int32_t* iters, const qpb_config* cfg, void* workspace,
+                         size_t workspace_bytes, qpb_stream_t stream);
+
+/* qpax/elastic_qp.py:381-417 diff_qp_elastic at iterate (x, t, s1, s2, lam1, lam2)
+ * -> (dQ, dq, dG, dh) cropped to the caller's blocks. */
+int qpb_diff_qp_elastic(const qpb_dims* dims, const double* Q, const double* q, const double* G,
+                        const double* h, const double* penalty, const double* const iterate[6],
+                        const double* dl_dx, double* dQ, double* dq, double* dG, double* dh,
+                        const qpb_config* cfg, void* workspace, size_t workspace_bytes, qpb_stream_t stream);
+
+/* Backward pass of qpax/elastic_qp.py:420-469 solve_qp_elastic_primal:
+ * relax_qp_elastic from the forward iterate, then diff_qp_elastic. */
+int qpb_solve_qp_elastic_primal_bwd(const qpb_dims* dims, const double* Q, const double* q, const double* G,
+                                    const double* h, const double* penalty, const double* const iterate[6],
+                                    const double* dl_dx, double solver_tol, double target_kappa, double* dQ,
+                                    double* dq, double* dG, double* dh, const qpb_config* cfg, void* workspace,
+                                    size_t workspace_bytes, qpb_stream_t stream);
+
+/* Human-readable name of a qpb_status code. */
+const char* qpb_status_string(int status);
+
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int32_t qpb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QPB_H_ */

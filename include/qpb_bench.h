@@ -1,0 +1,24 @@
+/*
+ * qpb_bench.h -- measurement helper exported by libqpb.so (no counterpart in
+ * qpax: it exists to put the solver's FP32/FP64 arithmetic next to the
+ * throughput the GPU can deliver).
+ */
+#ifndef QPB_BENCH_H_
+#define QPB_BENCH_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Runs a fused-multiply-add throughput kernel (independent FMA chains in
+ * every thread of a full grid) on `stream` and returns the achieved
+ * TFLOP/s (FMA = 2 FLOPs), or a negative value on a CUDA error.
+ * precision 0 = FP32, 1 = FP64.  `scratch` is a device buffer of at least
+ * 4 MiB that receives the chain results.  Synchronizes the stream. */
+double qpb_bench_fma_peak(int precision, void* scratch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QPB_BENCH_H_ */

@@ -41,6 +41,9 @@
 
 #define MAX_ITERS 30 /* qpax/pdip.py:232, pdip_relaxed.py:76, elastic_qp.py:195,325 */
 
+/* Optional per-iteration record of the KKT residual inf-norm (debug aid). */
+static __thread double *g_trace = NULL;
+
 /* ---------------------------------------------------------------- helpers */
 
 /* NaN-propagating min/max, as jnp.min / jnp.max behave. */
@@ -356,6 +359,7 @@ static int pdip_pc_step(kkt_t *K, step_ws_t *W, const double *Q, const double *q
   const int n = K->n, m = K->m, p = K->p;
   const double nrm = kkt_residuals(n, m, p, Q, q, A, b, G, h, x, s, z, y, 0.0, W->r1, W->r2, W->r3, W->r4, W->tmp_n);
   const int converged = (nrm < tol) ? 1 : 0;
+  if (g_trace) *g_trace++ = nrm;
   factorize_kkt(K, Q, G, A, s, z);
   for (int j = 0; j < n; j++) W->v1[j] = -W->r1[j];
   for (int i = 0; i < p; i++) W->v2[i] = -W->r2[i];
@@ -970,5 +974,16 @@ int oracle_diff_qp_elastic(int B, const int32_t *shapes, const double *Q, const 
                         z2 + o[i].p, dl_dx + o[i].n, dQ + o[i].Q, dq + o[i].q, dG + o[i].G, dh + o[i].h);
   }
   free(o);
+  return 0;
+}
+
+/* solve_qp on one instance, recording the residual inf-norm tested at each
+ * predictor-corrector iteration into trace[0..iters) (debug aid). */
+int oracle_solve_qp_trace(int n, int m, int p, const double *Q, const double *q, const double *A, const double *b,
+                          const double *G, const double *h, double tol, double *x, double *s, double *z, double *y,
+                          int32_t *conv, int32_t *iters, double *trace) {
+  g_trace = trace;
+  solve_qp_one(n, m, p, Q, q, A, b, G, h, tol, x, s, z, y, conv, iters);
+  g_trace = NULL;
   return 0;
 }

@@ -1,0 +1,439 @@
+// qpb_capi.cu -- persistent kernels, launch planning and the extern "C"
+// entry points declared in include/qpb.h.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/qpb.h"
+#include "qpb_kernel.cuh"
+
+namespace qpb {
+
+// ------------------------------------------------------------- planning
+constexpr size_t kCounterBytes = 256;
+constexpr int kMaxN = 256;
+
+struct Plan {
+  const void* fn;
+  int NT, threads, teams, grid;
+  size_t arena_bytes, smem_bytes, ws_bytes;
+  int in_smem;
+};
+
+static KernelFn pick_kernel(bool elastic, bool mixed, int NT, int KC) {
+  if (elastic) return mixed ? kernel_elastic_mixed(NT, KC) : kernel_elastic_f64(NT, KC);
+  return mixed ? kernel_std_mixed(NT, KC) : kernel_std_f64(NT, KC);
+}
+
+static int chunks_for(int k) {
+  const int c = (k + 31) / 32;
+  return c <= 1 ? 1 : c <= 2 ? 2 : c <= 4 ? 4 : 8;
+}
+
+static int auto_team(int n, int KC) {
+  if (KC >= 8) return 256;
+  if (KC >= 4) return n > 96 ? 256 : 128;
+  if (n <= 16) return 32;
+  return 128;
+}
+
+struct DevInfo {
+  int sms = 0, smem_optin = 0;
+  bool ok = false;
+};
+
+static DevInfo dev_info() {
+  static DevInfo cache[64];
+  static std::mutex mu;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DevInfo{};
+  std::lock_guard<std::mutex> lk(mu);
+  if (!cache[dev].ok) {
+    DevInfo d;
+    if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return DevInfo{};
+    if (cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+      return DevInfo{};
+    d.ok = true;
+    cache[dev] = d;
+  }
+  return cache[dev];
+}
+
+static int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
+  const bool elastic = op_is_elastic(op);
+  const bool mixed = cfg.precision == QPB_PRECISION_MIXED;
+  const int KC = chunks_for(d.n > d.m ? d.n : d.m);
+  int NT = cfg.team_threads ? cfg.team_threads : auto_team(d.n, KC);
+  if (NT == 32 && KC > 1) NT = 128;
+  if (NT == 128 && KC > 4) NT = 256;
+  if (NT == 256 && KC < 4) NT = 128;
+  KernelFn fn = pick_kernel(elastic, mixed, NT, KC);
+  if (!fn) return QPB_ERR_UNSUPPORTED;
+  const DevInfo di = dev_info();
+  if (!di.ok) return QPB_ERR_CUDA;
+  size_t arena = elastic ? ElasticArena::bytes(d.n, d.p, mixed) : StdArena::bytes(d.n, d.m, d.p, mixed);
+  arena = (arena + 255) & ~size_t(255);
+  pl->fn = (const void*)fn;
+  pl->NT = NT;
+  pl->arena_bytes = arena;
+  const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
+  int teams = 1;
+  if (NT == 32) {
+    // several warp teams per CTA, as many as fit (up to 8)
+    teams = (int)(smem_budget / arena);
+    teams = teams > 8 ? 8 : teams;
+  }
+  if (teams >= 1 && arena * teams <= smem_budget) {
+    pl->in_smem = 1;
+    pl->teams = teams;
+    pl->smem_bytes = arena * teams;
+  } else {
+    pl->in_smem = 0;
+    pl->teams = NT == 32 ? 4 : 1;
+    pl->smem_bytes = 0;
+  }
+  pl->threads = NT * pl->teams;
+  if (pl->smem_bytes > 48 * 1024) {
+    if (cudaFuncSetAttribute(pl->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem_bytes) !=
+        cudaSuccess)
+      return QPB_ERR_CUDA;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->fn, pl->threads, pl->smem_bytes) != cudaSuccess)
+    return QPB_ERR_CUDA;
+  if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
+  if (!pl->in_smem && per_sm > 2) per_sm = 2;
+  const long need = ((long)d.batch + pl->teams - 1) / pl->teams;
+  long grid = (long)per_sm * di.sms;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  pl->grid = (int)grid;
+  pl->ws_bytes = kCounterBytes + (pl->in_smem ? 0 : (size_t)grid * pl->teams * arena);
+  return QPB_OK;
+}
+
+static qpb_config resolve(const qpb_config* c) {
+  qpb_config r{};
+  if (c) r = *c;
+  if (r.pivot_max <= 0) r.pivot_max = 1e5;
+  if (r.max_sweeps <= 0) r.max_sweeps = 8;
+  return r;
+}
+
+static bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
+
+// Pointer check: required when count > 0.
+static bool ok_ptr(const void* p, long count) { return count == 0 || (p != nullptr && aligned8(p)); }
+
+static int check_common(int op, const qpb_dims* d, const qpb_config* cfg) {
+  if (!d) return QPB_ERR_INVALID_ARGUMENT;
+  if (d->batch < 0 || d->n < 1 || d->m < 0 || d->p < 0) return QPB_ERR_INVALID_ARGUMENT;
+  if (d->n > kMaxN || d->m > kMaxN) return QPB_ERR_UNSUPPORTED;
+  if (cfg) {
+    if (cfg->precision != QPB_PRECISION_MIXED && cfg->precision != QPB_PRECISION_FP64)
+      return QPB_ERR_INVALID_ARGUMENT;
+    if (cfg->team_threads != 0 && cfg->team_threads != 32 && cfg->team_threads != 128 && cfg->team_threads != 256)
+      return QPB_ERR_INVALID_ARGUMENT;
+    if (cfg->max_sweeps < 0 || cfg->max_sweeps > 64) return QPB_ERR_INVALID_ARGUMENT;
+    if (cfg->stats && !aligned8(cfg->stats) && (reinterpret_cast<uintptr_t>(cfg->stats) & 3))
+      return QPB_ERR_INVALID_ARGUMENT;
+  }
+  if (op_is_elastic(op)) {
+    if (d->m != 0) return QPB_ERR_INVALID_ARGUMENT;
+    if (d->p < 1) return QPB_ERR_UNSUPPORTED;
+  } else if (op != kOpSolve && op != kOpInit && d->p < 1) {
+    return QPB_ERR_UNSUPPORTED;  // qpax's relax/VJP cannot run without inequalities
+  }
+  return QPB_OK;
+}
+
+static int launch(Params P, const qpb_dims* d, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                  qpb_stream_t stream) {
+  const qpb_config c = resolve(cfg);
+  if (d->batch == 0) return QPB_OK;
+  Plan pl;
+  int st = make_plan(P.op, *d, c, &pl);
+  if (st != QPB_OK) return st;
+  if (!ws || ws_bytes < pl.ws_bytes || (reinterpret_cast<uintptr_t>(ws) & 255)) return QPB_ERR_WORKSPACE;
+  P.batch = d->batch;
+  P.n = d->n;
+  P.m = d->m;
+  P.p = d->p;
+  P.mixed = c.precision == QPB_PRECISION_MIXED;
+  P.pivot_max = c.pivot_max;
+  P.max_sweeps = c.max_sweeps;
+  P.stats = c.stats;
+  P.counter = reinterpret_cast<int*>(ws);
+  P.arena = reinterpret_cast<unsigned char*>(ws) + kCounterBytes;
+  P.arena_bytes = pl.arena_bytes;
+  P.arena_in_smem = pl.in_smem;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(ws, 0, sizeof(int), s) != cudaSuccess) return QPB_ERR_CUDA;
+  void* args[] = {&P};
+  if (cudaLaunchKernel(pl.fn, dim3(pl.grid), dim3(pl.threads), args, pl.smem_bytes, s) != cudaSuccess)
+    return QPB_ERR_CUDA;
+  return QPB_OK;
+}
+
+}  // namespace qpb
+
+using namespace qpb;
+
+extern "C" {
+
+int32_t qpb_version(void) { return 100; }
+
+const char* qpb_status_string(int status) {
+  switch (status) {
+    case QPB_OK: return "ok";
+    case QPB_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case QPB_ERR_UNSUPPORTED: return "unsupported shape or entry point";
+    case QPB_ERR_WORKSPACE: return "workspace too small or misaligned";
+    case QPB_ERR_CUDA: return "CUDA runtime error";
+    default: return "unknown status";
+  }
+}
+
+size_t qpb_workspace_size(int32_t op, const qpb_dims* dims, const qpb_config* cfg) {
+  if (check_common(op, dims, cfg) != QPB_OK) return 0;
+  const qpb_config c = resolve(cfg);
+  qpb_dims d = *dims;
+  if (d.batch == 0) return kCounterBytes;
+  Plan pl;
+  if (make_plan(op, d, c, &pl) != QPB_OK) return 0;
+  return pl.ws_bytes;
+}
+
+int qpb_solve_qp(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                 const double* G, const double* h, double solver_tol, double* x, double* s, double* z, double* y,
+                 int32_t* converged, int32_t* iters, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                 qpb_stream_t stream) {
+  int st = check_common(kOpSolve, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, m = d->m, p = d->p;
+  if (!ok_ptr(Q, B * n * n) || !ok_ptr(q, B * n) || !ok_ptr(A, B * m * n) || !ok_ptr(b, B * m) ||
+      !ok_ptr(G, B * p * n) || !ok_ptr(h, B * p) || !ok_ptr(x, B * n) || !ok_ptr(s, B * p) || !ok_ptr(z, B * p) ||
+      !ok_ptr(y, B * m) || (B && (!converged || !iters)))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpSolve;
+  P.tol = solver_tol;
+  P.Q = Q; P.q = q; P.A = A; P.b = b; P.G = G; P.h = h;
+  P.out[0] = x; P.out[1] = s; P.out[2] = z; P.out[3] = y;
+  P.conv = converged;
+  P.iters = iters;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_initialize(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                   const double* G, const double* h, double* x, double* s, double* z, double* y,
+                   const qpb_config* cfg, void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  int st = check_common(kOpInit, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, m = d->m, p = d->p;
+  if (!ok_ptr(Q, B * n * n) || !ok_ptr(q, B * n) || !ok_ptr(A, B * m * n) || !ok_ptr(b, B * m) ||
+      !ok_ptr(G, B * p * n) || !ok_ptr(h, B * p) || !ok_ptr(x, B * n) || !ok_ptr(s, B * p) || !ok_ptr(z, B * p) ||
+      !ok_ptr(y, B * m))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpInit;
+  P.Q = Q; P.q = q; P.A = A; P.b = b; P.G = G; P.h = h;
+  P.out[0] = x; P.out[1] = s; P.out[2] = z; P.out[3] = y;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_relax_qp(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                 const double* G, const double* h, const double* x_in, const double* s_in, const double* z_in,
+                 const double* y_in, double solver_tol, double target_kappa, double* x, double* s, double* z,
+                 double* y, int32_t* converged, int32_t* iters, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                 qpb_stream_t stream) {
+  int st = check_common(kOpRelax, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, m = d->m, p = d->p;
+  if (!ok_ptr(Q, B * n * n) || !ok_ptr(q, B * n) || !ok_ptr(A, B * m * n) || !ok_ptr(b, B * m) ||
+      !ok_ptr(G, B * p * n) || !ok_ptr(h, B * p) || !ok_ptr(x_in, B * n) || !ok_ptr(s_in, B * p) ||
+      !ok_ptr(z_in, B * p) || !ok_ptr(y_in, B * m) || !ok_ptr(x, B * n) || !ok_ptr(s, B * p) ||
+      !ok_ptr(z, B * p) || !ok_ptr(y, B * m) || (B && (!converged || !iters)))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpRelax;
+  P.tol = solver_tol;
+  P.kappa = target_kappa;
+  P.Q = Q; P.q = q; P.A = A; P.b = b; P.G = G; P.h = h;
+  P.in[0] = x_in; P.in[1] = s_in; P.in[2] = z_in; P.in[3] = y_in;
+  P.out[0] = x; P.out[1] = s; P.out[2] = z; P.out[3] = y;
+  P.conv = converged;
+  P.iters = iters;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_diff_qp(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                const double* G, const double* h, const double* x, const double* s, const double* lam,
+                const double* nu, const double* dl_dx, double* dQ, double* dq, double* dA, double* db, double* dG,
+                double* dh, const qpb_config* cfg, void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  int st = check_common(kOpAdjoint, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, m = d->m, p = d->p;
+  if (!ok_ptr(Q, B * n * n) || !ok_ptr(q, B * n) || !ok_ptr(A, B * m * n) || !ok_ptr(b, B * m) ||
+      !ok_ptr(G, B * p * n) || !ok_ptr(h, B * p) || !ok_ptr(x, B * n) || !ok_ptr(s, B * p) || !ok_ptr(lam, B * p) ||
+      !ok_ptr(nu, B * m) || !ok_ptr(dl_dx, B * n) || !ok_ptr(dQ, B * n * n) || !ok_ptr(dq, B * n) ||
+      !ok_ptr(dA, B * m * n) || !ok_ptr(db, B * m) || !ok_ptr(dG, B * p * n) || !ok_ptr(dh, B * p))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpAdjoint;
+  P.Q = Q; P.q = q; P.A = A; P.b = b; P.G = G; P.h = h;
+  P.in[0] = x; P.in[1] = s; P.in[2] = lam; P.in[3] = nu;
+  P.gx = dl_dx;
+  P.dQ = dQ; P.dq = dq; P.dA = dA; P.db = db; P.dG = dG; P.dh = dh;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_solve_qp_primal_bwd(const qpb_dims* d, const double* Q, const double* q, const double* A,
+                            const double* b, const double* G, const double* h, const double* x, const double* s,
+                            const double* z, const double* y, const double* dl_dx, double solver_tol,
+                            double target_kappa, double* dQ, double* dq, double* dA, double* db, double* dG,
+                            double* dh, double* xr, double* sr, double* zr, double* yr, int32_t* converged,
+                            int32_t* iters, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                            qpb_stream_t stream) {
+  int st = check_common(kOpBwd, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, m = d->m, p = d->p;
+  const bool want_iter = xr != nullptr;
+  if (!ok_ptr(Q, B * n * n) || !ok_ptr(q, B * n) || !ok_ptr(A, B * m * n) || !ok_ptr(b, B * m) ||
+      !ok_ptr(G, B * p * n) || !ok_ptr(h, B * p) || !ok_ptr(x, B * n) || !ok_ptr(s, B * p) || !ok_ptr(z, B * p) ||
+      !ok_ptr(y, B * m) || !ok_ptr(dl_dx, B * n) || !ok_ptr(dQ, B * n * n) || !ok_ptr(dq, B * n) ||
+      !ok_ptr(dA, B * m * n) || !ok_ptr(db, B * m) || !ok_ptr(dG, B * p * n) || !ok_ptr(dh, B * p))
+    return QPB_ERR_INVALID_ARGUMENT;
+  if (want_iter && (!ok_ptr(xr, B * n) || !ok_ptr(sr, B * p) || !ok_ptr(zr, B * p) || !ok_ptr(yr, B * m)))
+    return QPB_ERR_INVALID_ARGUMENT;
+  if (!ok_ptr(converged, 0) || !ok_ptr(iters, 0)) return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpBwd;
+  P.tol = solver_tol;
+  P.kappa = target_kappa;
+  P.Q = Q; P.q = q; P.A = A; P.b = b; P.G = G; P.h = h;
+  P.in[0] = x; P.in[1] = s; P.in[2] = z; P.in[3] = y;
+  P.gx = dl_dx;
+  if (want_iter) {
+    P.out[0] = xr; P.out[1] = sr; P.out[2] = zr; P.out[3] = yr;
+  }
+  P.conv = converged;
+  P.iters = iters;
+  P.dQ = dQ; P.dq = dq; P.dA = dA; P.db = db; P.dG = dG; P.dh = dh;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+static bool ok_elastic_inputs(const qpb_dims* d, const double* Q, const double* q, const double* G,
+                              const double* h, const double* pen) {
+  const long B = d->batch, n = d->n, p = d->p;
+  return ok_ptr(Q, B * n * n) && ok_ptr(q, B * n) && ok_ptr(G, B * p * n) && ok_ptr(h, B * p) && ok_ptr(pen, B);
+}
+
+static bool ok_iterate6(const qpb_dims* d, const double* const it[6]) {
+  if (!it) return d->batch == 0;
+  const long B = d->batch, n = d->n, p = d->p;
+  if (!ok_ptr(it[0], B * n)) return false;
+  for (int k = 1; k < 6; ++k)
+    if (!ok_ptr(it[k], B * p)) return false;
+  return true;
+}
+
+int qpb_solve_qp_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,
+                         const double* penalty, double solver_tol, double* x, double* t, double* s1, double* s2,
+                         double* z1, double* z2, int32_t* converged, int32_t* iters, const qpb_config* cfg,
+                         void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  int st = check_common(kOpESolve, d, cfg);
+  if (st) return st;
+  double* out[6] = {x, t, s1, s2, z1, z2};
+  if (!ok_elastic_inputs(d, Q, q, G, h, penalty) || !ok_iterate6(d, out) ||
+      (d->batch && (!converged || !iters)))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpESolve;
+  P.tol = solver_tol;
+  P.Q = Q; P.q = q; P.G = G; P.h = h; P.penalty = penalty;
+  for (int k = 0; k < 6; ++k) P.out[k] = out[k];
+  P.conv = converged;
+  P.iters = iters;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_initialize_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,
+                           const double* penalty, double* x, double* t, double* s1, double* s2, double* z1,
+                           double* z2, const qpb_config* cfg, void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  int st = check_common(kOpEInit, d, cfg);
+  if (st) return st;
+  double* out[6] = {x, t, s1, s2, z1, z2};
+  if (!ok_elastic_inputs(d, Q, q, G, h, penalty) || !ok_iterate6(d, out)) return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpEInit;
+  P.Q = Q; P.q = q; P.G = G; P.h = h; P.penalty = penalty;
+  for (int k = 0; k < 6; ++k) P.out[k] = out[k];
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_relax_qp_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,
+                         const double* penalty, const double* const iterate_in[6], double solver_tol,
+                         double target_kappa, double* const iterate_out[6], int32_t* converged, int32_t* iters,
+                         const qpb_config* cfg, void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  int st = check_common(kOpERelax, d, cfg);
+  if (st) return st;
+  if (!ok_elastic_inputs(d, Q, q, G, h, penalty) || !ok_iterate6(d, iterate_in) ||
+      !ok_iterate6(d, (const double* const*)iterate_out) || (d->batch && (!converged || !iters)))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpERelax;
+  P.tol = solver_tol;
+  P.kappa = target_kappa;
+  P.Q = Q; P.q = q; P.G = G; P.h = h; P.penalty = penalty;
+  for (int k = 0; k < 6 && d->batch; ++k) {
+    P.in[k] = iterate_in[k];
+    P.out[k] = iterate_out[k];
+  }
+  P.conv = converged;
+  P.iters = iters;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_diff_qp_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,
+                        const double* penalty, const double* const iterate[6], const double* dl_dx, double* dQ,
+                        double* dq, double* dG, double* dh, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                        qpb_stream_t stream) {
+  int st = check_common(kOpEAdjoint, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, p = d->p;
+  if (!ok_elastic_inputs(d, Q, q, G, h, penalty) || !ok_iterate6(d, iterate) || !ok_ptr(dl_dx, B * n) ||
+      !ok_ptr(dQ, B * n * n) || !ok_ptr(dq, B * n) || !ok_ptr(dG, B * p * n) || !ok_ptr(dh, B * p))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpEAdjoint;
+  P.Q = Q; P.q = q; P.G = G; P.h = h; P.penalty = penalty;
+  for (int k = 0; k < 6 && B; ++k) P.in[k] = iterate[k];
+  P.gx = dl_dx;
+  P.dQ = dQ; P.dq = dq; P.dG = dG; P.dh = dh;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+int qpb_solve_qp_elastic_primal_bwd(const qpb_dims* d, const double* Q, const double* q, const double* G,
+                                    const double* h, const double* penalty, const double* const iterate[6],
+                                    const double* dl_dx, double solver_tol, double target_kappa, double* dQ,
+                                    double* dq, double* dG, double* dh, const qpb_config* cfg, void* ws,
+                                    size_t ws_bytes, qpb_stream_t stream) {
+  int st = check_common(kOpEBwd, d, cfg);
+  if (st) return st;
+  const long B = d->batch, n = d->n, p = d->p;
+  if (!ok_elastic_inputs(d, Q, q, G, h, penalty) || !ok_iterate6(d, iterate) || !ok_ptr(dl_dx, B * n) ||
+      !ok_ptr(dQ, B * n * n) || !ok_ptr(dq, B * n) || !ok_ptr(dG, B * p * n) || !ok_ptr(dh, B * p))
+    return QPB_ERR_INVALID_ARGUMENT;
+  Params P{};
+  P.op = kOpEBwd;
+  P.tol = solver_tol;
+  P.kappa = target_kappa;
+  P.Q = Q; P.q = q; P.G = G; P.h = h; P.penalty = penalty;
+  for (int k = 0; k < 6 && B; ++k) P.in[k] = iterate[k];
+  P.gx = dl_dx;
+  P.dQ = dQ; P.dq = dq; P.dG = dG; P.dh = dh;
+  return launch(P, d, cfg, ws, ws_bytes, stream);
+}
+
+}  // extern "C"

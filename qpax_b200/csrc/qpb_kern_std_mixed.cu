@@ -1,0 +1,14 @@
+// Kernel instantiations: StdQP, FP32 factor + FP64 refinement.
+#include "qpb_kernel.cuh"
+
+namespace qpb {
+
+KernelFn kernel_std_mixed(int NT, int KC) {
+#define QPB_ENTRY(nt, kc) \
+  if (NT == nt && KC == kc) return ipm_kernel<StdQP<nt, kc, true>, nt>;
+  QPB_FOR_EACH_VARIANT(QPB_ENTRY)
+#undef QPB_ENTRY
+  return nullptr;
+}
+
+}  // namespace qpb

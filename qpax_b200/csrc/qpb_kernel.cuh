@@ -1,0 +1,52 @@
+// qpb_kernel.cuh -- the persistent interior-point kernel template and the
+// per-translation-unit kernel tables.
+#pragma once
+#include "qpb_elastic.cuh"
+#include "qpb_std.cuh"
+
+namespace qpb {
+
+// Persistent: each team pulls instance indices from P.counter until the
+// batch is exhausted (a bounded loop: at most `batch` fetches in total).
+template <class Solver, int NT>
+__global__ void __launch_bounds__(256) ipm_kernel(const __grid_constant__ Params P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int next_inst;
+  const int teams = blockDim.x / NT;
+  const int team = threadIdx.x / NT;
+  const int rank = threadIdx.x - team * NT;
+  unsigned char* arena = P.arena_in_smem
+                             ? smem + (size_t)team * P.arena_bytes
+                             : P.arena + ((size_t)blockIdx.x * teams + team) * P.arena_bytes;
+  Solver S;
+  S.setup(P, arena, rank);
+  for (;;) {
+    int inst;
+    if constexpr (NT == 32) {
+      int v = 0;
+      if (rank == 0) v = atomicAdd(P.counter, 1);
+      inst = __shfl_sync(kFull, v, 0);
+    } else {
+      if (rank == 0) next_inst = atomicAdd(P.counter, 1);
+      __syncthreads();
+      inst = next_inst;
+      __syncthreads();
+    }
+    if (inst >= P.batch) break;
+    S.run(inst);
+  }
+}
+
+using KernelFn = void (*)(Params);
+
+// Kernel for (team threads NT, register chunks KC); nullptr if not built.
+KernelFn kernel_std_f64(int NT, int KC);
+KernelFn kernel_std_mixed(int NT, int KC);
+KernelFn kernel_elastic_f64(int NT, int KC);
+KernelFn kernel_elastic_mixed(int NT, int KC);
+
+// (NT, KC) variants compiled into the library.
+#define QPB_FOR_EACH_VARIANT(X) X(32, 1) X(128, 1) X(128, 2) X(128, 4) X(256, 4) X(256, 8)
+
+
+}  // namespace qpb

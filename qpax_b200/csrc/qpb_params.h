@@ -1,0 +1,51 @@
+// qpb_params.h -- launch parameters shared by the host launcher and kernels.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+namespace qpb {
+
+enum Op : int {
+  kOpSolve = 0,    // solve_qp                     qpax/pdip.py:181-251
+  kOpInit = 1,     // initialize                   qpax/pdip.py:15-35
+  kOpRelax = 2,    // relax_qp                     qpax/pdip_relaxed.py:70-103
+  kOpBwd = 3,      // relax_qp + diff_qp           qpax/diff_qp.py:61-79
+  kOpAdjoint = 4,  // diff_qp                      qpax/diff_qp.py:20-46
+  kOpESolve = 5,   // solve_qp_elastic             qpax/elastic_qp.py:184-228
+  kOpEInit = 6,    // initialize_elastic           qpax/elastic_qp.py:27-47
+  kOpERelax = 7,   // relax_qp_elastic             qpax/elastic_qp.py:319-359
+  kOpEBwd = 8,     // relax_qp_elastic + diff_qp_elastic  qpax/elastic_qp.py:433-466
+  kOpEAdjoint = 9  // diff_qp_elastic              qpax/elastic_qp.py:381-417
+};
+
+inline bool op_is_elastic(int op) { return op >= kOpESolve; }
+
+// Per-instance statistics (optional output, 4 int32 per instance).
+enum Stat : int { kStatFact32 = 0, kStatFact64 = 1, kStatSweeps = 2, kStatFlags = 3 };
+enum Flag : int {
+  kFlagFallback = 1,      // FP32 factor rejected at least once -> FP64 refactor
+  kFlagRefineStall = 2,   // refinement did not reach FP64 accuracy in the sweep limit
+  kFlagBreakdown64 = 4,   // FP64 factor had a non-positive pivot (outputs follow IEEE arithmetic)
+  kFlagNonFinite = 8      // a non-finite value reached the iterate
+};
+
+struct Params {
+  int op, batch, n, m, p;
+  int mixed;            // 0: FP64 factor; 1: FP32 factor + FP64 refinement
+  double tol, kappa;
+  double pivot_max;     // mixed: FP32 factor rejected when max(d)/min(d) exceeds this
+  int max_sweeps;       // mixed: refinement sweeps before falling back to FP64
+  const double *Q, *q, *A, *b, *G, *h, *penalty;
+  const double *in[6];  // starting iterate: (x,s,z,y) or elastic (x,t,s1,s2,z1,z2)
+  const double *gx;     // incoming gradient dl/dx
+  double *out[6];       // iterate out (same order)
+  int32_t *conv, *iters;
+  double *dQ, *dq, *dA, *db, *dG, *dh;
+  int32_t *stats;       // optional
+  unsigned char *arena; // global arenas when they do not fit in shared memory
+  size_t arena_bytes;   // bytes per team arena
+  int arena_in_smem;
+  int *counter;         // work counter (zeroed before launch)
+};
+
+}  // namespace qpb
