@@ -40,7 +40,11 @@ typedef enum {
   QPB_ERR_CUDA = 4              /* a CUDA runtime call failed (launch, attributes) */
 } qpb_status;
 
-typedef enum { QPB_PRECISION_MIXED = 0, QPB_PRECISION_FP64 = 1 } qpb_precision;
+/* AUTO picks, per problem size, the fastest path that meets FP64 accuracy:
+ * today the FP64 kernels (one warp per instance for n <= 32, m <= n_pad/4;
+ * one CTA per instance above).  MIXED forces FP32 factorisation with FP64
+ * refinement; FP64 forces FP64 factorisation. */
+typedef enum { QPB_PRECISION_AUTO = 0, QPB_PRECISION_MIXED = 1, QPB_PRECISION_FP64 = 2 } qpb_precision;
 
 typedef enum {
   QPB_OP_SOLVE = 0,
@@ -64,8 +68,9 @@ typedef struct {
 
 /* Optional tuning; pass NULL for defaults. */
 typedef struct {
-  int32_t precision;    /* qpb_precision; default QPB_PRECISION_MIXED */
-  int32_t team_threads; /* threads per instance: 0 = automatic, 32, 128 or 256 */
+  int32_t precision;    /* qpb_precision; default QPB_PRECISION_AUTO */
+  int32_t team_threads; /* threads per instance: 0 = automatic, 32, 128 or 256
+                           (128/256 force the one-CTA-per-instance kernel) */
   double pivot_max;     /* mixed: FP32 factor used while max(d)/min(d) <= pivot_max (0 = 1e5) */
   int32_t max_sweeps;   /* mixed: FP64 refinement sweeps per solve before FP64 refactor (0 = 8) */
   int32_t* stats;       /* optional device int32[batch][4]: FP32 factorisations, FP64

@@ -20,7 +20,7 @@ OPS = {
     "solve": 0, "initialize": 1, "relax": 2, "primal_bwd": 3, "diff": 4,
     "elastic_solve": 5, "elastic_initialize": 6, "elastic_relax": 7, "elastic_primal_bwd": 8, "elastic_diff": 9,
 }
-PRECISION = {"mixed": 0, "fp64": 1}
+PRECISION = {"auto": 0, "mixed": 1, "fp64": 2}
 
 _lock = threading.Lock()
 _lib = None
@@ -107,7 +107,7 @@ def ptr(t) -> int | None:
     return t.data_ptr() if t.numel() else None
 
 
-def make_config(precision: str = "mixed", team_threads: int = 0, pivot_max: float = 0.0, max_sweeps: int = 0,
+def make_config(precision: str = "auto", team_threads: int = 0, pivot_max: float = 0.0, max_sweeps: int = 0,
                 stats: torch.Tensor | None = None) -> Config:
     if precision not in PRECISION:
         raise ValueError(f"precision must be one of {sorted(PRECISION)}")

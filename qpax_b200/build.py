@@ -28,6 +28,7 @@ SOURCES = [
     "qpb_kern_std_mixed.cu",
     "qpb_kern_elastic_f64.cu",
     "qpb_kern_elastic_mixed.cu",
+    "qpb_kern_warp.cu",
     "qpb_bench.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

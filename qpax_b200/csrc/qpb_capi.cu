@@ -6,6 +6,7 @@
 
 #include "../../include/qpb.h"
 #include "qpb_kernel.cuh"
+#include "qpb_warp.cuh"
 
 namespace qpb {
 
@@ -59,9 +60,54 @@ static DevInfo dev_info() {
   return cache[dev];
 }
 
+// Padded column count of the one-warp-per-instance kernel, or 0 when the
+// instance does not fit it (n <= 32, m <= NP / 4).
+static int warp_np(const qpb_dims& d) {
+  const int np = d.n <= 8 ? 8 : d.n <= 16 ? 16 : d.n <= 32 ? 32 : 0;
+  return (np && d.m <= np / 4) ? np : 0;
+}
+
 static int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   const bool elastic = op_is_elastic(op);
   const bool mixed = cfg.precision == QPB_PRECISION_MIXED;
+  const DevInfo di = dev_info();
+  if (!di.ok) return QPB_ERR_CUDA;
+  const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
+  const int np = warp_np(d);
+  if (!elastic && !mixed && np && (cfg.team_threads == 0 || cfg.team_threads == 32)) {
+    // one warp per instance, FP64, several instances per CTA
+    KernelFn fn = kernel_warp_f64(np);
+    if (!fn) return QPB_ERR_UNSUPPORTED;
+    size_t arena = (WarpArena::bytes(np, np / 4, d.p) + 255) & ~size_t(255);
+    pl->fn = (const void*)fn;
+    pl->NT = 32;
+    pl->arena_bytes = arena;
+    pl->teams = kWarpKernelThreads / 32;
+    pl->threads = kWarpKernelThreads;
+    if (arena * pl->teams <= smem_budget) {
+      pl->in_smem = 1;
+      pl->smem_bytes = arena * pl->teams;
+    } else {
+      pl->in_smem = 0;
+      pl->smem_bytes = 0;
+    }
+    if (pl->smem_bytes > 48 * 1024 &&
+        cudaFuncSetAttribute(pl->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem_bytes) !=
+            cudaSuccess)
+      return QPB_ERR_CUDA;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->fn, pl->threads, pl->smem_bytes) !=
+        cudaSuccess)
+      return QPB_ERR_CUDA;
+    if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
+    if (!pl->in_smem && per_sm > 4) per_sm = 4;
+    const long need = ((long)d.batch + pl->teams - 1) / pl->teams;
+    long grid = (long)per_sm * di.sms;
+    grid = grid > need ? need : grid;
+    pl->grid = (int)(grid < 1 ? 1 : grid);
+    pl->ws_bytes = kCounterBytes + (pl->in_smem ? 0 : (size_t)pl->grid * pl->teams * arena);
+    return QPB_OK;
+  }
   const int KC = chunks_for(d.n > d.m ? d.n : d.m);
   int NT = cfg.team_threads ? cfg.team_threads : auto_team(d.n, KC);
   if (NT == 32 && KC > 1) NT = 128;
@@ -69,14 +115,11 @@ static int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl)
   if (NT == 256 && KC < 4) NT = 128;
   KernelFn fn = pick_kernel(elastic, mixed, NT, KC);
   if (!fn) return QPB_ERR_UNSUPPORTED;
-  const DevInfo di = dev_info();
-  if (!di.ok) return QPB_ERR_CUDA;
   size_t arena = elastic ? ElasticArena::bytes(d.n, d.p, mixed) : StdArena::bytes(d.n, d.m, d.p, mixed);
   arena = (arena + 255) & ~size_t(255);
   pl->fn = (const void*)fn;
   pl->NT = NT;
   pl->arena_bytes = arena;
-  const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
   int teams = 1;
   if (NT == 32) {
     // several warp teams per CTA, as many as fit (up to 8)
@@ -130,7 +173,8 @@ static int check_common(int op, const qpb_dims* d, const qpb_config* cfg) {
   if (d->batch < 0 || d->n < 1 || d->m < 0 || d->p < 0) return QPB_ERR_INVALID_ARGUMENT;
   if (d->n > kMaxN || d->m > kMaxN) return QPB_ERR_UNSUPPORTED;
   if (cfg) {
-    if (cfg->precision != QPB_PRECISION_MIXED && cfg->precision != QPB_PRECISION_FP64)
+    if (cfg->precision != QPB_PRECISION_AUTO && cfg->precision != QPB_PRECISION_MIXED &&
+        cfg->precision != QPB_PRECISION_FP64)
       return QPB_ERR_INVALID_ARGUMENT;
     if (cfg->team_threads != 0 && cfg->team_threads != 32 && cfg->team_threads != 128 && cfg->team_threads != 256)
       return QPB_ERR_INVALID_ARGUMENT;

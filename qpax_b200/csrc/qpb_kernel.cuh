@@ -44,6 +44,9 @@ KernelFn kernel_std_f64(int NT, int KC);
 KernelFn kernel_std_mixed(int NT, int KC);
 KernelFn kernel_elastic_f64(int NT, int KC);
 KernelFn kernel_elastic_mixed(int NT, int KC);
+// One warp per instance, n <= NP (8, 16, 32), m <= NP / 4; FP64.
+KernelFn kernel_warp_f64(int NP);
+constexpr int kWarpKernelThreads = 128;
 
 // (NT, KC) variants compiled into the library.
 #define QPB_FOR_EACH_VARIANT(X) X(32, 1) X(128, 1) X(128, 2) X(128, 4) X(256, 4) X(256, 8)

@@ -18,11 +18,11 @@ import torch
 from . import _lib
 from ._lib import Dims, as_f64, ptr
 
-DEFAULTS = {"precision": "mixed", "team_threads": 0, "pivot_max": 0.0, "max_sweeps": 0}
+DEFAULTS = {"precision": "auto", "team_threads": 0, "pivot_max": 0.0, "max_sweeps": 0}
 
 
 def set_defaults(**kw) -> None:
-    """Set library-wide defaults for precision ('mixed' | 'fp64'), team_threads,
+    """Set library-wide defaults for precision ('auto' | 'mixed' | 'fp64'), team_threads,
     pivot_max and max_sweeps (see include/qpb.h qpb_config)."""
     for k, v in kw.items():
         if k not in DEFAULTS:

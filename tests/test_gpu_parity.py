@@ -4,7 +4,11 @@ Bars (written per assertion):
   x, s, z, y, t, s1, s2, z1, z2: ||gpu - oracle||_inf <= 1e-6 * max(1, ||oracle||_inf) per instance
   gradients:                     ||gpu - oracle||_inf <= 1e-5 * max(1, ||oracle||_inf) per instance and array
   converged flags:               identical; iteration counts: identical
-for both precision modes ("fp64": FP64 factor; "mixed": FP32 factor + FP64 refinement).
+for each kernel family:
+  "auto":     the default dispatch (one warp per instance in FP64 for n <= 32, m <= n_pad/4,
+              one CTA per instance in FP64 above)
+  "fp64-cta": one CTA per instance, FP64 factor (the plain FP64 kernel)
+  "mixed":    one CTA per instance, FP32 factor + FP64 refinement + FP64 fallback
 """
 
 import numpy as np
@@ -17,7 +21,12 @@ from tests.refgen import batch_random_qps, kkt_inf_norms
 
 pytestmark = pytest.mark.gpu
 
-PRECS = ["fp64", "mixed"]
+VARIANTS = {
+    "auto": dict(precision="auto"),
+    "fp64-cta": dict(precision="fp64", team_threads=128),
+    "mixed": dict(precision="mixed"),
+}
+PRECS = list(VARIANTS)
 X_TOL = 1e-6
 G_TOL = 1e-5
 
@@ -59,7 +68,7 @@ def check_solve(Q, q, A, b, G, h, tol, prec, max_breakdown=0.0, **kw):
     such instances is bounded by max_breakdown."""
     import qpax_b200 as qb
 
-    out = qb.solve_qp(Q, q, A, b, G, h, tol, precision=prec, **kw)
+    out = qb.solve_qp(Q, q, A, b, G, h, tol, **VARIANTS[prec], **kw)
     ref = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=tol)
     ok = np.atleast_1d(ref[4]) == 1
     assert (~ok).mean() <= max_breakdown, f"reference breakdowns {(~ok).sum()} of {ok.size}"
@@ -99,7 +108,7 @@ def _vjp_pair(Q, q, A, b, G, h, tol, kappa, prec):
 
     x_ref = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=tol)[0]
     dl = wl.loss_grad(x_ref)
-    x, grads, conv, iters = qb.solve_qp_primal_vjp(Q, q, A, b, G, h, dl, tol, kappa, precision=prec)
+    x, grads, conv, iters = qb.solve_qp_primal_vjp(Q, q, A, b, G, h, dl, tol, kappa, **VARIANTS[prec])
     x_o, grads_o, conv_o, iters_o = oracle.solve_qp_primal_vjp(Q, q, A, b, G, h, dl, solver_tol=tol,
                                                               target_kappa=kappa)
     return (x, grads, conv, iters), (x_o, grads_o, conv_o, iters_o)
@@ -160,7 +169,7 @@ def test_constraint_sizes(pins, prec):
                  "test_QPTEST"]:
         d = _pin(pins, f"sizes/{name}")
         args = [d[k] for k in ("Q", "q", "A", "b", "G", "h")]
-        x, s, z, y, conv, iters = (np_(t) for t in qb.solve_qp(*args, float(d["solver_tol"]), precision=prec))
+        x, s, z, y, conv, iters = (np_(t) for t in qb.solve_qp(*args, float(d["solver_tol"]), **VARIANTS[prec]))
         ref = oracle.solve_qp(*args, solver_tol=float(d["solver_tol"]))
         assert int(conv) == int(ref[4]) == 1, name
         assert int(iters) == int(ref[5]), name
@@ -181,9 +190,9 @@ def test_elastic_golden(pins, prec):
 
     P, I = _pin(pins, "elastic/problem_data_pos"), _pin(pins, "elastic/initial_values_pos")
     args = (P["Q"], P["q"], P["G"], P["h"], float(P["penalty"]))
-    for k, v in zip(("x", "t", "s1", "s2", "z1", "z2"), qb.initialize_elastic(*args, precision=prec)):
+    for k, v in zip(("x", "t", "s1", "s2", "z1", "z2"), qb.initialize_elastic(*args, **VARIANTS[prec])):
         assert np.linalg.norm(np_(v) - I[k]) < 1e-6, k
-    out = qb.solve_qp_elastic(*args, solver_tol=1e-10, precision=prec)
+    out = qb.solve_qp_elastic(*args, solver_tol=1e-10, **VARIANTS[prec])
     assert int(out[6]) == 1
     for k, v in zip(("x", "t", "s1", "s2", "z1", "z2"), out[:6]):
         assert np.linalg.norm(np_(v) - P[k]) < 1e-6, k
@@ -195,7 +204,7 @@ def test_elastic_configuration5(prec):
     import qpax_b200 as qb
 
     Q, q, G, h, bad = wl.elastic(64)
-    out = qb.solve_qp_elastic(Q, q, G, h, 1e3, 1e-6, precision=prec)
+    out = qb.solve_qp_elastic(Q, q, G, h, 1e3, 1e-6, **VARIANTS[prec])
     ref = oracle.solve_qp_elastic(Q, q, G, h, 1e3, solver_tol=1e-6)
     ok = ref[6] == 1
     assert (~ok).mean() <= 0.1
@@ -215,7 +224,7 @@ def test_elastic_gradients(prec):
     Q, q, G, h, _ = wl.elastic(32, seed=55, n=12, p=24, pairs=2)
     x_ref = oracle.solve_qp_elastic(Q, q, G, h, 50.0, solver_tol=1e-6)[0]
     dl = wl.loss_grad(x_ref)
-    x, grads = qb.solve_qp_elastic_primal_vjp(Q, q, G, h, 50.0, dl, 1e-6, 1e-3, precision=prec)
+    x, grads = qb.solve_qp_elastic_primal_vjp(Q, q, G, h, 50.0, dl, 1e-6, 1e-3, **VARIANTS[prec])
     x_o, grads_o = oracle.solve_qp_elastic_primal_vjp(Q, q, G, h, 50.0, dl, solver_tol=1e-6, target_kappa=1e-3)
     assert_close(x, x_o, X_TOL, "x")
     # qpax's elastic relaxation (elastic_qp.py:255-261) uses residual signs
@@ -237,13 +246,13 @@ def test_elastic_vjp_vs_augmented_vjp(pins, prec):
     Q, q, G, h, pen = P["Q"], P["q"], P["G"], P["h"], float(P["penalty"])
     n, p = len(q), len(h)
     x_des = np.random.default_rng(0).standard_normal(n)
-    x = np_(qb.solve_qp_elastic(Q, q, G, h, pen, 1e-6, precision=prec)[0])
-    _, g1 = qb.solve_qp_elastic_primal_vjp(Q, q, G, h, pen, 2 * (x - x_des), 1e-6, 1e-3, precision=prec)
+    x = np_(qb.solve_qp_elastic(Q, q, G, h, pen, 1e-6, **VARIANTS[prec])[0])
+    _, g1 = qb.solve_qp_elastic_primal_vjp(Q, q, G, h, pen, 2 * (x - x_des), 1e-6, 1e-3, **VARIANTS[prec])
     Q2, q2, A2, b2, G2, h2 = augmented_problem(Q, q, G, h, pen)
-    x2 = np_(qb.solve_qp(Q2, q2, A2, b2, G2, h2, 1e-6, precision=prec)[0])
+    x2 = np_(qb.solve_qp(Q2, q2, A2, b2, G2, h2, 1e-6, **VARIANTS[prec])[0])
     dl = np.concatenate((2 * (x2[:n] - x_des), np.zeros(p)))
     _, (dQ2, dq2, _, _, dG2, dh2), _, _ = qb.solve_qp_primal_vjp(Q2, q2, A2, b2, G2, h2, dl, 1e-6, 1e-3,
-                                                                 precision=prec)
+                                                                 **VARIANTS[prec])
     g2 = (np_(dQ2)[:n, :n], np_(dq2)[:n], np_(dG2)[p:, :n], np_(dh2)[p:])
     for a, b_ in zip(g1, g2):
         assert np.linalg.norm(np_(a) - b_) < 1e-3
