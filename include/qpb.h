@@ -159,6 +159,30 @@ int qpb_solve_qp_elastic_primal_bwd(const qpb_dims* dims, const double* Q, const
                                     double* dq, double* dG, double* dh, const qpb_config* cfg, void* workspace,
                                     size_t workspace_bytes, qpb_stream_t stream);
 
+/* qpb_solve_qp for callers that cannot allocate device memory.  No
+ * counterpart in qpax: it exists for hosts where a solve must not call
+ * cudaMalloc -- code recorded into a CUDA graph whose capture forbids
+ * allocation, real-time loops that allocate everything at start-up, plugins
+ * whose framework owns the device allocator and offers no workspace hook.
+ * Same arguments and results as qpb_solve_qp, minus the workspace: the
+ * scratch (the persistent launch's work counter, and the global arena of
+ * instances too large for shared memory) comes from a 1 MiB array that the
+ * library keeps in device memory on every GPU that loads it, until the
+ * process exits.  Problems whose qpb_workspace_size exceeds 1 MiB are
+ * rejected with QPB_ERR_UNSUPPORTED; every problem whose instances fit in
+ * shared memory (all n <= 32; up to about n = 64 when p = 2n) needs only
+ * 256 bytes of it, for any batch size.
+ * Nothing is allocated, by this call or by the library on its behalf.  The
+ * first call on a device looks up the array's device address (one-time
+ * set-up), so make that first call before any stream capture.  All calls
+ * share the one array: calls that may overlap on the GPU (different streams
+ * without ordering between them) race on it and must be serialised by the
+ * caller; calls on one stream are safe. */
+int qpb_solve_qp_noalloc(const qpb_dims* dims, const double* Q, const double* q, const double* A,
+                         const double* b, const double* G, const double* h, double solver_tol, double* x,
+                         double* s, double* z, double* y, int32_t* converged, int32_t* iters,
+                         const qpb_config* cfg, qpb_stream_t stream);
+
 /* Human-readable name of a qpb_status code. */
 const char* qpb_status_string(int status);
 

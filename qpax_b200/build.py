@@ -30,6 +30,7 @@ SOURCES = [
     "qpb_kern_elastic_mixed.cu",
     "qpb_kern_warp.cu",
     "qpb_bench.cu",
+    "qpb_noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE]
