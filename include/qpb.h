@@ -159,6 +159,44 @@ int qpb_solve_qp_elastic_primal_bwd(const qpb_dims* dims, const double* Q, const
                                     double* dq, double* dG, double* dh, const qpb_config* cfg, void* workspace,
                                     size_t workspace_bytes, qpb_stream_t stream);
 
+/* ---- Uneven batches ----------------------------------------------------
+ * A qpax user with instances of different shapes runs one jit(vmap(solve_qp))
+ * per shape (qpax/pdip.py:208-217 branch on Python shapes).  Here one call
+ * serves them all: instance i has its own (n_i, m_i, p_i), p_i >= 1, and each
+ * array is the concatenation of the per-instance row-major arrays in instance
+ * order (Q_0 Q_1 ... ; q_0 q_1 ... ; likewise A, b, G, h and the outputs).
+ * A plan groups the instances by kernel variant once (host side, allocating
+ * its small index tables and streams); each call then runs one persistent
+ * launch per size bin, forked from `stream` onto the plan's streams and
+ * joined back, so a CUDA graph captures the call whole.  A plan belongs to
+ * the device current at its creation; calls sharing a plan must not overlap. */
+typedef struct qpb_plan_st qpb_plan;
+
+/* shapes: host int32[batch][3] = (n, m, p).  cfg as for the uniform calls. */
+int qpb_plan_create(qpb_plan** plan, int32_t batch, const int32_t* shapes, const qpb_config* cfg);
+int qpb_plan_destroy(qpb_plan* plan);
+/* Workspace bytes a call with this plan needs (every op). */
+size_t qpb_plan_workspace_size(const qpb_plan* plan);
+/* Number of size bins (persistent launches per call). */
+int32_t qpb_plan_num_bins(const qpb_plan* plan);
+/* Packed lengths (elements) of Q, q, A, b, G, h. */
+int qpb_plan_totals(const qpb_plan* plan, int64_t totals[6]);
+
+/* qpax/pdip.py:181-251 solve_qp over a packed batch (outputs packed like q, h, h, b). */
+int qpb_solve_qp_packed(const qpb_plan* plan, const double* Q, const double* q, const double* A, const double* b,
+                        const double* G, const double* h, double solver_tol, double* x, double* s, double* z,
+                        double* y, int32_t* converged, int32_t* iters, void* workspace, size_t workspace_bytes,
+                        qpb_stream_t stream);
+
+/* qpax/diff_qp.py:74-79 backward of solve_qp_primal over a packed batch
+ * (gradients packed like Q, q, A, b, G, h). */
+int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const double* q, const double* A,
+                                   const double* b, const double* G, const double* h, const double* x,
+                                   const double* s, const double* z, const double* y, const double* dl_dx,
+                                   double solver_tol, double target_kappa, double* dQ, double* dq, double* dA,
+                                   double* db, double* dG, double* dh, void* workspace, size_t workspace_bytes,
+                                   qpb_stream_t stream);
+
 /* qpb_solve_qp for callers that cannot allocate device memory.  No
  * counterpart in qpax: it exists for hosts where a solve must not call
  * cudaMalloc -- code recorded into a CUDA graph whose capture forbids

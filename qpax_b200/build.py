@@ -31,6 +31,7 @@ SOURCES = [
     "qpb_kern_warp.cu",
     "qpb_bench.cu",
     "qpb_noalloc.cu",
+    "qpb_plan.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE]

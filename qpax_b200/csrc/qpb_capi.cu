@@ -5,28 +5,20 @@
 #include <mutex>
 
 #include "../../include/qpb.h"
+#include "qpb_host.h"
 #include "qpb_kernel.cuh"
-#include "qpb_warp.cuh"
+#include "qpb_warpqp.cuh"
 
 namespace qpb {
 
 // ------------------------------------------------------------- planning
-constexpr size_t kCounterBytes = 256;
-constexpr int kMaxN = 256;
-
-struct Plan {
-  const void* fn;
-  int NT, threads, teams, grid;
-  size_t arena_bytes, smem_bytes, ws_bytes;
-  int in_smem;
-};
 
 static KernelFn pick_kernel(bool elastic, bool mixed, int NT, int KC) {
   if (elastic) return mixed ? kernel_elastic_mixed(NT, KC) : kernel_elastic_f64(NT, KC);
   return mixed ? kernel_std_mixed(NT, KC) : kernel_std_f64(NT, KC);
 }
 
-static int chunks_for(int k) {
+int chunks_for(int k) {
   const int c = (k + 31) / 32;
   return c <= 1 ? 1 : c <= 2 ? 2 : c <= 4 ? 4 : 8;
 }
@@ -62,12 +54,12 @@ static DevInfo dev_info() {
 
 // Padded column count of the one-warp-per-instance kernel, or 0 when the
 // instance does not fit it (n <= 32, m <= NP / 4).
-static int warp_np(const qpb_dims& d) {
+int warp_np(const qpb_dims& d) {
   const int np = d.n <= 8 ? 8 : d.n <= 16 ? 16 : d.n <= 32 ? 32 : 0;
   return (np && d.m <= np / 4) ? np : 0;
 }
 
-static int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
+int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   const bool elastic = op_is_elastic(op);
   const bool mixed = cfg.precision == QPB_PRECISION_MIXED;
   const DevInfo di = dev_info();
@@ -155,7 +147,7 @@ static int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl)
   return QPB_OK;
 }
 
-static qpb_config resolve(const qpb_config* c) {
+qpb_config resolve_config(const qpb_config* c) {
   qpb_config r{};
   if (c) r = *c;
   if (r.pivot_max <= 0) r.pivot_max = 1e5;
@@ -166,9 +158,9 @@ static qpb_config resolve(const qpb_config* c) {
 static bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
 
 // Pointer check: required when count > 0.
-static bool ok_ptr(const void* p, long count) { return count == 0 || (p != nullptr && aligned8(p)); }
+bool ok_ptr(const void* p, long count) { return count == 0 || (p != nullptr && aligned8(p)); }
 
-static int check_common(int op, const qpb_dims* d, const qpb_config* cfg) {
+int check_common(int op, const qpb_dims* d, const qpb_config* cfg) {
   if (!d) return QPB_ERR_INVALID_ARGUMENT;
   if (d->batch < 0 || d->n < 1 || d->m < 0 || d->p < 0) return QPB_ERR_INVALID_ARGUMENT;
   if (d->n > kMaxN || d->m > kMaxN) return QPB_ERR_UNSUPPORTED;
@@ -193,7 +185,7 @@ static int check_common(int op, const qpb_dims* d, const qpb_config* cfg) {
 
 static int launch(Params P, const qpb_dims* d, const qpb_config* cfg, void* ws, size_t ws_bytes,
                   qpb_stream_t stream) {
-  const qpb_config c = resolve(cfg);
+  const qpb_config c = resolve_config(cfg);
   if (d->batch == 0) return QPB_OK;
   Plan pl;
   int st = make_plan(P.op, *d, c, &pl);
@@ -240,7 +232,7 @@ const char* qpb_status_string(int status) {
 
 size_t qpb_workspace_size(int32_t op, const qpb_dims* dims, const qpb_config* cfg) {
   if (check_common(op, dims, cfg) != QPB_OK) return 0;
-  const qpb_config c = resolve(cfg);
+  const qpb_config c = resolve_config(cfg);
   qpb_dims d = *dims;
   if (d.batch == 0) return kCounterBytes;
   Plan pl;

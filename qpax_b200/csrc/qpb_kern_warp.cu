@@ -1,6 +1,6 @@
 // Kernel instantiations: one warp per instance (n <= 32, m <= n_pad / 4), FP64.
 #include "qpb_kernel.cuh"
-#include "qpb_warp.cuh"
+#include "qpb_warpqp.cuh"
 
 namespace qpb {
 

@@ -46,6 +46,42 @@ struct Params {
   size_t arena_bytes;   // bytes per team arena
   int arena_in_smem;
   int *counter;         // work counter (zeroed before launch)
+  // Packed (uneven) batches: when `shapes` is set, instance i has its own
+  // (n, m, p) = shapes[3i..3i+2] and element offsets offs[6i..6i+5] into the
+  // packed Q, q, A, b, G, h arrays (x, dq, gx follow q; y, db follow b; s, z,
+  // dh follow h; dQ, dA, dG follow Q, A, G).  `list` names the instances of
+  // this launch (one size bin); the launch covers list[0 .. batch).
+  const int32_t *shapes;
+  const int64_t *offs;
+  const int32_t *list;
 };
+
+// Where instance `inst` (a launch-local index) lives.
+struct InstRef {
+  long id;                       // instance index in the whole batch
+  long oQ, oq, oA, ob, oG, oh;   // element offsets
+  int n, m, p;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ InstRef inst_ref(const Params& P, long i) {
+  InstRef r;
+  if (P.shapes) {
+    const long id = P.list ? P.list[i] : i;
+    r.id = id;
+    r.n = P.shapes[3 * id];
+    r.m = P.shapes[3 * id + 1];
+    r.p = P.shapes[3 * id + 2];
+    const int64_t* o = P.offs + 6 * id;
+    r.oQ = o[0]; r.oq = o[1]; r.oA = o[2]; r.ob = o[3]; r.oG = o[4]; r.oh = o[5];
+  } else {
+    r.id = i;
+    r.n = P.n; r.m = P.m; r.p = P.p;
+    r.oQ = i * (long)P.n * P.n; r.oq = i * (long)P.n; r.oA = i * (long)P.m * P.n;
+    r.ob = i * (long)P.m; r.oG = i * (long)P.p * P.n; r.oh = i * (long)P.p;
+  }
+  return r;
+}
+#endif
 
 }  // namespace qpb

@@ -49,11 +49,14 @@ struct StdQP {
   StdArena a;
   const Params* P;
   int n, m, p, ld;
+  InstRef R;                 // the instance being solved
+  unsigned char* arena_base;
 
   QPB_DEV const Team<NT>& t() const { return k.t; }
 
   QPB_DEV void setup(const Params& prm, unsigned char* arena, int rank) {
     P = &prm;
+    arena_base = arena;
     n = prm.n; m = prm.m; p = prm.p;
     a.carve(reinterpret_cast<uintptr_t>(arena), n, m, p, kMixed);
     ld = a.ld;
@@ -70,10 +73,11 @@ struct StdQP {
   // +-inf get h = 0 and a zero row of G (qpax/pdip.py:166-178).
   QPB_NOINLINE void load(long inst, bool remove_inf) {
     const Team<NT>& T = t();
-    const double* gQ = P->Q + inst * (long)n * n;
-    const double* gG = P->G + inst * (long)p * n;
-    const double* gA = P->A + inst * (long)m * n;
-    const double* gh = P->h + inst * (long)p;
+    (void)inst;
+    const double* gQ = P->Q + R.oQ;
+    const double* gG = P->G + R.oG;
+    const double* gA = P->A + R.oA;
+    const double* gh = P->h + R.oh;
     for (int e = T.r; e < n * ld; e += NT) {
       const int i = e / ld, j = e - i * ld;
       a.Q[e] = (j < n) ? gQ[(long)i * n + j] : 0.0;
@@ -88,9 +92,9 @@ struct StdQP {
       const int i = e / ld, j = e - i * ld;
       a.A[e] = (j < n) ? gA[(long)i * n + j] : 0.0;
     }
-    for (int i = T.r; i < n; i += NT) a.q[i] = P->q[inst * n + i];
+    for (int i = T.r; i < n; i += NT) a.q[i] = P->q[R.oq + i];
     for (int i = T.r; i < m; i += NT) {
-      a.b[i] = P->b[inst * m + i];
+      a.b[i] = P->b[R.ob + i];
       a.zm[i] = 0.0;
     }
     for (int i = T.r; i < p; i += NT) {
@@ -112,28 +116,30 @@ struct StdQP {
 
   QPB_NOINLINE void load_iterate(long inst) {
     const Team<NT>& T = t();
-    for (int i = T.r; i < n; i += NT) a.x[i] = P->in[0][inst * n + i];
+    (void)inst;
+    for (int i = T.r; i < n; i += NT) a.x[i] = P->in[0][R.oq + i];
     for (int i = T.r; i < p; i += NT) {
-      a.s[i] = P->in[1][inst * p + i];
-      a.z[i] = P->in[2][inst * p + i];
+      a.s[i] = P->in[1][R.oh + i];
+      a.z[i] = P->in[2][R.oh + i];
     }
-    for (int i = T.r; i < m; i += NT) a.y[i] = P->in[3][inst * m + i];
+    for (int i = T.r; i < m; i += NT) a.y[i] = P->in[3][R.ob + i];
     T.sync();
   }
 
   QPB_NOINLINE void store_iterate(long inst, bool inf_rows) {
     const Team<NT>& T = t();
-    for (int i = T.r; i < n; i += NT) P->out[0][inst * n + i] = a.x[i];
+    (void)inst;
+    for (int i = T.r; i < n; i += NT) P->out[0][R.oq + i] = a.x[i];
     for (int i = T.r; i < p; i += NT) {
       double sv = a.s[i], zv = a.z[i];
-      if (inf_rows && isinf(P->h[inst * p + i])) {  // qpax/pdip.py:243-246
+      if (inf_rows && isinf(P->h[R.oh + i])) {  // qpax/pdip.py:243-246
         zv = 0.0;
         sv = INFINITY;
       }
-      P->out[1][inst * p + i] = sv;
-      P->out[2][inst * p + i] = zv;
+      P->out[1][R.oh + i] = sv;
+      P->out[2][R.oh + i] = zv;
     }
-    for (int i = T.r; i < m; i += NT) P->out[3][inst * m + i] = a.y[i];
+    for (int i = T.r; i < m; i += NT) P->out[3][R.ob + i] = a.y[i];
   }
 
   // qpax/pdip.py:49-63 solve_kkt_rhs for right-hand sides (c1, c2, c3, c4).
@@ -281,35 +287,46 @@ struct StdQP {
   QPB_NOINLINE void adjoint(long inst) {
     const Team<NT>& T = t();
     for (int i = T.r; i < p; i += NT) a.w[i] = a.z[i] / a.s[i];
-    for (int j = T.r; j < n; j += NT) a.v1[j] = -P->gx[inst * n + j];
+    (void)inst;
+    for (int j = T.r; j < n; j += NT) a.v1[j] = -P->gx[R.oq + j];
     T.sync();
     k.use64 = 0;
     k.factor();
     solve(a.v1, a.zp, a.zp, a.zm, a.dx, a.ds, a.dz, a.dy);
     for (int i = T.r; i < p; i += NT) a.dz[i] = a.dz[i] / a.z[i];  // dlam = dlam_tilde / lam
     T.sync();
-    double* dQ = P->dQ + inst * (long)n * n;
+    double* dQ = P->dQ + R.oQ;
     for (int e = T.r; e < n * n; e += NT) {
       const int i = e / n, j = e - i * n;
       dQ[e] = 0.5 * (a.dx[i] * a.x[j] + a.x[i] * a.dx[j]);
     }
-    double* dA = P->dA + inst * (long)m * n;
+    double* dA = P->dA + R.oA;
     for (int e = T.r; e < m * n; e += NT) {
       const int i = e / n, j = e - i * n;
       dA[e] = a.dy[i] * a.x[j] + a.y[i] * a.dx[j];
     }
-    double* dG = P->dG + inst * (long)p * n;
+    double* dG = P->dG + R.oG;
     for (int e = T.r; e < p * n; e += NT) {
       const int i = e / n, j = e - i * n;
       dG[e] = a.z[i] * (a.dz[i] * a.x[j] + a.z[i] * a.dx[j]);
     }
-    for (int j = T.r; j < n; j += NT) P->dq[inst * n + j] = a.dx[j];
-    for (int i = T.r; i < m; i += NT) P->db[inst * m + i] = -a.dy[i];
-    for (int i = T.r; i < p; i += NT) P->dh[inst * p + i] = -a.z[i] * a.dz[i];
+    for (int j = T.r; j < n; j += NT) P->dq[R.oq + j] = a.dx[j];
+    for (int i = T.r; i < m; i += NT) P->db[R.ob + i] = -a.dy[i];
+    for (int i = T.r; i < p; i += NT) P->dh[R.oh + i] = -a.z[i] * a.dz[i];
   }
 
-  QPB_NOINLINE void run(long inst) {
+  QPB_NOINLINE void run(long i) {
     const Team<NT>& T = t();
+    R = inst_ref(*P, i);
+    const long inst = R.id;
+    if (P->shapes) {  // packed batch: this instance's shapes and arena layout
+      n = R.n; m = R.m; p = R.p;
+      a.carve(reinterpret_cast<uintptr_t>(arena_base), n, m, p, kMixed);
+      ld = a.ld;
+      k.n = n; k.m = m; k.p = p; k.ld = ld;
+      k.c = a;
+      k.t.red = a.red;
+    }
     k.reset_stats();
     const int op = P->op;
     int conv = 0, iters = 0;

@@ -1,0 +1,554 @@
+// qpb_warpqp.cuh -- one warp per QP instance for n <= NP (NP = 8, 16, 32),
+// m <= MP = NP / 4, any p; FP64 throughout.
+//
+// Same method and formula order as qpb_std.cuh (qpax/pdip.py, pdip_relaxed.py,
+// diff_qp.py; citations there), laid out for a single warp so that no phase
+// needs a block-wide barrier:
+//   * lane j owns column j of H = Q + G' diag(w) G in registers (hc[NP]) and
+//     factors it in place (LDL^T, right-looking, one shared-memory broadcast
+//     of the pivot row per step).  Afterwards lane j holds column j of L
+//     (scaled by d_j) below the diagonal and row j of L (scaled by d_i) above
+//     it, which is exactly what column-oriented forward and backward
+//     substitution need from that lane;
+//   * Y = L^-1 A' is formed in registers (lane j holds Y[:, j]) and kept in
+//     shared memory with the m x m Schur complement F = Y' D^-1 Y and its
+//     factor;
+//   * n- and m-vectors are lane-distributed registers; p-vectors and the G,
+//     A operands live in shared memory; Q is read through L1/L2.
+// Every solve of the instance -- initial point, predictor, corrector, Newton
+// step of the relaxation, adjoint -- runs through one factor() and one
+// solve() call site (run() is a bounded state machine), which keeps the
+// unrolled code small enough for the instruction cache.
+#pragma once
+#include "qpb_params.h"
+#include "qpb_team.cuh"
+
+namespace qpb {
+
+QPB_DEV double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+QPB_DEV double wmax(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = nmax(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+QPB_DEV double wmin(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = nmin(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Shared-memory layout of one warp instance (doubles, in this order):
+//   G (p x NP) | A (MP x NP) | 9 p-vectors | xs, cb, dvi (NP each) |
+//   Y (MP x NP, Y[i][j] = (L^-1 A')[j][i]) | F (MP x MP, column-held factor)
+// Addresses are recomputed from the base and p where used (no pointer table).
+struct WarpArena {
+  static __host__ __device__ size_t doubles(int NP, int MP, int p) {
+    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + 3 * (size_t)NP + (size_t)MP * NP +
+           (size_t)MP * MP;
+  }
+  static size_t bytes(int NP, int MP, int p) { return doubles(NP, MP, p) * sizeof(double) + 16; }
+};
+
+enum WarpSlot : int { kVh = 0, kVs, kVz, kVw, kVv2, kVv3, kVds, kVdz, kVtp };
+
+template <int NP, int MP>
+struct WarpAddr {
+  double* base;
+  int p;
+  QPB_DEV double* G() const { return base; }
+  QPB_DEV double* A() const { return base + p * NP; }
+  QPB_DEV double* v(int k) const { return base + p * NP + MP * NP + k * p; }
+  QPB_DEV double* h() const { return v(kVh); }
+  QPB_DEV double* s() const { return v(kVs); }
+  QPB_DEV double* z() const { return v(kVz); }
+  QPB_DEV double* w() const { return v(kVw); }
+  QPB_DEV double* v2() const { return v(kVv2); }
+  QPB_DEV double* v3() const { return v(kVv3); }
+  QPB_DEV double* ds() const { return v(kVds); }
+  QPB_DEV double* dz() const { return v(kVdz); }
+  QPB_DEV double* tp() const { return v(kVtp); }
+  QPB_DEV double* xs() const { return base + p * NP + MP * NP + 9 * p; }
+  QPB_DEV double* cb() const { return xs() + NP; }
+  QPB_DEV double* dvi() const { return xs() + 2 * NP; }
+  QPB_DEV double* Y() const { return xs() + 3 * NP; }
+  QPB_DEV double* F() const { return Y() + MP * NP; }
+};
+
+template <int NP, int MP>
+struct WarpQP {
+  static_assert(NP == 8 || NP == 16 || NP == 32, "NP");
+  const Params* P;
+  WarpAddr<NP, MP> a;
+  int n, m, p, lane;
+  const double* gQ;  // this instance's Q (row-major n x n, global)
+  double hc[NP];     // H column -> L, D (lane-owned column)
+  double dinv;       // 1 / d_lane
+  double fdinv;      // 1 / df_lane (lanes < MP)
+  double x, q;       // n-vectors (lane j)
+  double y, b;       // m-vectors (lane i)
+  int st_f64, st_flags;
+
+  QPB_DEV void setup(const Params& prm, unsigned char* arena, int ln) {
+    P = &prm;
+    n = prm.n; m = prm.m; p = prm.p;
+    lane = ln;
+    a.base = reinterpret_cast<double*>(arena);
+    a.p = p;
+  }
+
+  // sym(Q)[i][lane] through L1 (Q is symmetrized on the fly: (Q + Q')/2).
+  QPB_DEV double qsym(int i) const {
+    return (i < n && lane < n) ? 0.5 * (gQ[i * n + lane] + gQ[lane * n + i]) : 0.0;
+  }
+
+  QPB_DEV void load(const InstRef& R, bool remove_inf) {
+    gQ = P->Q + R.oQ;
+    const double* gG = P->G + R.oG;
+    const double* gA = P->A + R.oA;
+    const double* gh = P->h + R.oh;
+    for (int r = 0; r < p; ++r) {
+      double v = (lane < n) ? gG[r * n + lane] : 0.0;
+      if (remove_inf && isinf(gh[r])) v = 0.0;
+      if (lane < NP) a.G()[r * NP + lane] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < MP; ++i)
+      if (lane < NP) a.A()[i * NP + lane] = (i < m && lane < n) ? gA[i * n + lane] : 0.0;
+    for (int r = lane; r < p; r += 32) {
+      const double hv = gh[r];
+      a.h()[r] = (remove_inf && isinf(hv)) ? 0.0 : hv;
+    }
+    q = (lane < n) ? P->q[R.oq + lane] : 0.0;
+    b = (lane < m) ? P->b[R.ob + lane] : 0.0;
+    __syncwarp();
+  }
+
+  QPB_DEV void load_iterate(const InstRef& R) {
+    x = (lane < n) ? P->in[0][R.oq + lane] : 0.0;
+    y = (lane < m) ? P->in[3][R.ob + lane] : 0.0;
+    for (int r = lane; r < p; r += 32) {
+      a.s()[r] = P->in[1][R.oh + r];
+      a.z()[r] = P->in[2][R.oh + r];
+    }
+    __syncwarp();
+  }
+
+  QPB_DEV void store_iterate(const InstRef& R, bool inf_rows) {
+    if (lane < n) P->out[0][R.oq + lane] = x;
+    if (lane < m) P->out[3][R.ob + lane] = y;
+    for (int r = lane; r < p; r += 32) {
+      double sv = a.s()[r], zv = a.z()[r];
+      if (inf_rows && isinf(P->h[R.oh + r])) {  // qpax/pdip.py:243-246
+        zv = 0.0;
+        sv = INFINITY;
+      }
+      P->out[1][R.oh + r] = sv;
+      P->out[2][R.oh + r] = zv;
+    }
+  }
+
+  // ---------------------------------------------------------------- factor
+  // H = sym(Q) + G' diag(w) G (w in shared memory), LDL^T in registers,
+  // then Y = L^-1 A' and F = Y D^-1 Y' with its LDL^T in shared memory.
+  QPB_DEV void factor() {
+    st_f64++;
+    dinv = 0.0;
+    fdinv = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qsym(i);
+    const double* Gc = a.G() + (lane < NP ? lane : 0);
+    const double* wv = a.w();
+    for (int r = 0; r < p; ++r) {
+      const double* row = a.G() + r * NP;
+      const double ar = (lane < NP) ? wv[r] * Gc[r * NP] : 0.0;
+#pragma unroll
+      for (int i = 0; i < NP; i += 2) {
+        const double2 g2 = *reinterpret_cast<const double2*>(row + i);
+        hc[i] = fma(g2.x, ar, hc[i]);
+        hc[i + 1] = fma(g2.y, ar, hc[i + 1]);
+      }
+    }
+    // LDL^T: step k broadcasts row k of the Schur complement (= column k)
+    int bad = 0;
+    double* cb = a.cb();
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      if (lane < NP) cb[lane] = hc[k];
+      __syncwarp();
+      const double dk = cb[k];
+      const double rk = 1.0 / dk;
+      if (k < n) bad |= !(dk > 0.0) || !isfinite(dk);
+      if (lane == k) dinv = rk;
+      const double f = hc[k] * rk;
+      if (lane > k) {
+#pragma unroll
+        for (int i = k + 1; i < NP; ++i) hc[i] = fma(-cb[i], f, hc[i]);
+      }
+      __syncwarp();
+    }
+    if (lane < NP) a.dvi()[lane] = dinv;
+    __syncwarp();
+    // Y = L^-1 A'   (unit L; L[j][k] = hc[k] * dinv_k for lane j > k)
+    double yc[MP];
+#pragma unroll
+    for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
+#pragma unroll
+    for (int k = 0; k < NP - 1; ++k) {
+      const double l = (lane > k && lane < NP) ? hc[k] * a.dvi()[k] : 0.0;
+#pragma unroll
+      for (int i = 0; i < MP; ++i) yc[i] = fma(-l, __shfl_sync(kFull, yc[i], k), yc[i]);
+    }
+    if (lane < NP) {
+#pragma unroll
+      for (int i = 0; i < MP; ++i) a.Y()[i * NP + lane] = yc[i];
+    }
+    __syncwarp();
+    // F = Y D^-1 Y' (MP x MP, full storage, identity beyond m), one entry per lane
+    double* Fm = a.F();
+    const double* Ys = a.Y();
+    const double* dv = a.dvi();
+    for (int e = lane; e < MP * MP; e += 32) {
+      const int r = e / MP, c = e - r * MP;
+      double v = (r == c) ? 1.0 : 0.0;
+      if (r < m && c < m) {
+        double acc = 0.0;
+#pragma unroll 8
+        for (int j = 0; j < NP; ++j) acc = fma(Ys[r * NP + j] * dv[j], Ys[c * NP + j], acc);
+        v = acc;
+      }
+      Fm[e] = v;
+    }
+    __syncwarp();
+    // LDL^T of F in the same in-place layout as H: lane c owns column c
+    for (int k = 0; k < MP; ++k) {
+      const double dk = Fm[k * MP + k];
+      const double rk = 1.0 / dk;
+      if (k < m) bad |= !(dk > 0.0) || !isfinite(dk);
+      if (lane == k) fdinv = rk;
+      if (lane > k && lane < MP) {
+        const double f = Fm[k * MP + lane] * rk;
+        for (int i = k + 1; i < MP; ++i) Fm[i * MP + lane] = fma(-Fm[i * MP + k], f, Fm[i * MP + lane]);
+      }
+      __syncwarp();
+    }
+    if (bad) st_flags |= kFlagBreakdown64;
+  }
+
+  QPB_DEV double ycol(int i) const { return lane < NP ? a.Y()[i * NP + lane] : 0.0; }
+  QPB_DEV double fcol(int k) const { return lane < MP ? a.F()[k * MP + lane] : 0.0; }
+
+  // --------------------------------------------------------- reduced solve
+  // [H A'; A 0][dx; dy] = [r; v]  (r lane j < n, v lane i < m)
+  QPB_DEV void reduced(double r, double v, double& odx, double& ody) {
+    double u = (lane < n) ? r : 0.0;  // u = L^-1 r
+#pragma unroll
+    for (int k = 0; k < NP - 1; ++k) {
+      const double uk = __shfl_sync(kFull, u, k) * a.dvi()[k];
+      if (lane > k) u = fma(-hc[k], uk, u);
+    }
+    const double ud = (lane < NP) ? u * dinv : 0.0;
+    double g = 0.0;
+#pragma unroll
+    for (int i = 0; i < MP; ++i) {
+      const double gi = wsum(ycol(i) * ud);
+      if (lane == i) g = gi - v;
+    }
+    if (lane >= m) g = 0.0;
+    // dy = F^-1 g: forward (lane i > k holds Lf[i][k] df_k in column slot k)
+#pragma unroll
+    for (int k = 0; k < MP - 1; ++k) {
+      const double gk = __shfl_sync(kFull, g, k) * __shfl_sync(kFull, fdinv, k);
+      if (lane > k && lane < MP) g = fma(-fcol(k), gk, g);
+    }
+    g = (lane < MP) ? g * fdinv : 0.0;
+    // backward (lane i < k holds Lf[k][i] df_i in slot k)
+#pragma unroll
+    for (int k = MP - 1; k > 0; --k) {
+      const double gk = __shfl_sync(kFull, g, k);
+      if (lane < k) g = fma(-fcol(k) * fdinv, gk, g);
+    }
+    ody = (lane < m) ? g : 0.0;
+    // dx = L^-T D^-1 (u - Y dy)
+    double wv = u;
+#pragma unroll
+    for (int i = 0; i < MP; ++i) wv = fma(-ycol(i), __shfl_sync(kFull, g, i), wv);
+    double xv = (lane < NP) ? wv * dinv : 0.0;
+#pragma unroll
+    for (int k = NP - 1; k > 0; --k) {
+      const double xk = __shfl_sync(kFull, xv, k);
+      if (lane < k) xv = fma(-hc[k] * dinv, xk, xv);  // L[k][i] = hc[k] dinv_i in lane i
+    }
+    odx = (lane < n) ? xv : 0.0;
+  }
+
+  // Row dots G x with x in xs (rotated walk: conflict-free shared reads).
+  QPB_DEV double grow_dot(int r, const double* xsv) const {
+    const double* row = a.G() + r * NP;
+    double g0 = 0.0, g1 = 0.0;
+#pragma unroll
+    for (int t = 0; t < NP; t += 2) {
+      const int c0 = (t + r) & (NP - 1), c1 = (t + 1 + r) & (NP - 1);
+      g0 = fma(row[c0], xsv[c0], g0);
+      g1 = fma(row[c1], xsv[c1], g1);
+    }
+    return g0 + g1;
+  }
+
+  // Column dots G' v (v in shared memory, length p), lane j.
+  QPB_DEV double gcol_dot(const double* vv) const {
+    const double* Gc = a.G() + (lane < NP ? lane : 0);
+    double acc0 = 0.0, acc1 = 0.0;
+    int r = 0;
+    for (; r + 2 <= p; r += 2) {
+      acc0 = fma(Gc[r * NP], vv[r], acc0);
+      acc1 = fma(Gc[(r + 1) * NP], vv[r + 1], acc1);
+    }
+    if (r < p) acc0 = fma(Gc[r * NP], vv[r], acc0);
+    return acc0 + acc1;
+  }
+
+  // ------------------------------------------------------------ KKT solve
+  // qpax/pdip.py:49-63.  With slack == false the right-hand side is the
+  // reduced one directly ([H A'; A 0][dx; dy] = [c1; c4], qpax/pdip.py:22-24).
+  QPB_DEV void solve(bool slack, double c1, const double* c2, const double* c3, double c4, double& odx,
+                     double& ody) {
+    double p1 = c1;
+    if (slack) {
+      double* tp = a.tp();
+      for (int r = lane; r < p; r += 32) tp[r] = a.w()[r] * (c3[r] - c2[r] / a.z()[r]);
+      __syncwarp();
+      p1 = (lane < n) ? c1 + gcol_dot(tp) : 0.0;
+    }
+    reduced(p1, c4, odx, ody);
+    if (slack) {
+      if (lane < NP) a.xs()[lane] = odx;
+      __syncwarp();
+      double* ds = a.ds();
+      double* dz = a.dz();
+      for (int r = lane; r < p; r += 32) {
+        const double dsr = c3[r] - grow_dot(r, a.xs());
+        ds[r] = dsr;
+        dz[r] = (c2[r] - a.z()[r] * dsr) / a.s()[r];
+      }
+      __syncwarp();
+    }
+  }
+
+  // -(relaxed KKT residuals): v1, v4 returned in registers, v2, v3 and
+  // w = z/s in shared memory; returns the inf-norm.
+  // qpax/pdip.py:93-100, pdip_relaxed.py:16-23.
+  QPB_DEV double residuals(double kappa, double& v1, double& v4) {
+    double qx = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) qx = fma(qsym(i), __shfl_sync(kFull, x, i), qx);
+    double ay = 0.0;
+#pragma unroll
+    for (int i = 0; i < MP; ++i) ay = fma(ycol_a(i), __shfl_sync(kFull, y, i), ay);
+    const double r1 = ((qx + q) + ay) + gcol_dot(a.z());
+    double loc = (lane < n) ? fabs(r1) : 0.0;
+    v1 = (lane < n) ? -r1 : 0.0;
+    if (lane < NP) a.xs()[lane] = x;
+    __syncwarp();
+    double r4 = 0.0;
+#pragma unroll
+    for (int i = 0; i < MP; ++i) {
+      const double ax = wsum(ycol_a(i) * x);
+      if (lane == i) r4 = ax - b;
+    }
+    v4 = (lane < m) ? -r4 : 0.0;
+    if (lane < m) loc = nmax(loc, fabs(r4));
+    for (int r = lane; r < p; r += 32) {
+      const double sr = a.s()[r], zr = a.z()[r];
+      const double r3 = (grow_dot(r, a.xs()) + sr) - a.h()[r];
+      const double r2 = sr * zr - kappa;
+      a.v3()[r] = -r3;
+      a.v2()[r] = -r2;
+      a.w()[r] = zr / sr;
+      loc = nmax(loc, nmax(fabs(r3), fabs(r2)));
+    }
+    __syncwarp();
+    return wmax(loc);
+  }
+
+  QPB_DEV double ycol_a(int i) const { return lane < NP ? a.A()[i * NP + lane] : 0.0; }
+
+  // min over the lane's entries of -v/d for d < 0 (qpax/pdip.py:66-73 before the cap).
+  QPB_DEV double ls_local(const double* v, const double* d) const {
+    double mn = INFINITY;
+    for (int r = lane; r < p; r += 32) {
+      const double dr = d[r];
+      if (dr < 0) mn = nmin(mn, -v[r] / dr);
+    }
+    return mn;
+  }
+
+  // qpax/diff_qp.py:20-46 optnet_derivatives :8-17, from the adjoint solution.
+  QPB_DEV void write_grads(const InstRef& R, double ddx, double ddy) {
+    for (int r = lane; r < p; r += 32) a.dz()[r] = a.dz()[r] / a.z()[r];  // dlam = dlam_tilde / lam
+    __syncwarp();
+    double* dQ = P->dQ + R.oQ;
+    for (int i = 0; i < n; ++i) {
+      const double dxi = __shfl_sync(kFull, ddx, i), xi = __shfl_sync(kFull, x, i);
+      if (lane < n) dQ[i * n + lane] = 0.5 * (dxi * x + xi * ddx);
+    }
+    double* dA = P->dA + R.oA;
+    for (int i = 0; i < m; ++i) {
+      const double dyi = __shfl_sync(kFull, ddy, i), yi = __shfl_sync(kFull, y, i);
+      if (lane < n) dA[i * n + lane] = dyi * x + yi * ddx;
+    }
+    double* dG = P->dG + R.oG;
+    for (int r = 0; r < p; ++r) {
+      const double lam = a.z()[r], dl = a.dz()[r];
+      if (lane < n) dG[r * n + lane] = lam * (dl * x + lam * ddx);
+    }
+    if (lane < n) P->dq[R.oq + lane] = ddx;
+    if (lane < m) P->db[R.ob + lane] = -ddy;
+    for (int r = lane; r < p; r += 32) P->dh[R.oh + r] = -a.z()[r] * a.dz()[r];
+  }
+
+  // --------------------------------------------------------------- driver
+  enum Stage : int { kInit, kStep, kCorrector, kAdjoint, kDone };
+
+  QPB_DEV void run(long i) {
+    st_f64 = st_flags = 0;
+    const InstRef R = inst_ref(*P, i);
+    n = R.n;
+    m = R.m;
+    p = R.p;
+    a.p = p;
+    const long inst = R.id;
+    const int op = P->op;
+    const bool relaxed = (op == kOpRelax || op == kOpBwd);
+    load(R, op == kOpSolve);
+    int stage;
+    if (op == kOpSolve || op == kOpInit) {
+      stage = kInit;
+    } else {
+      load_iterate(R);
+      stage = (op == kOpAdjoint) ? kAdjoint : kStep;
+    }
+    if (op == kOpSolve && p == 0) stage = kInit;
+    int it = 0, converged = 0, conv_now = 0;
+    double v1 = 0.0, v4 = 0.0, dxr = 0.0, dyr = 0.0;
+    double sigma_mu = 0.0;
+    // bounded: initial point + 2 solves per iteration + adjoint
+    for (int guard = 0; guard < 2 * kMaxIters + 4 && stage != kDone; ++guard) {
+      // ---- prepare the system: weights, right-hand side, factor or not
+      bool slack = true, refactor = true;
+      double c1 = 0.0, c4 = 0.0;
+      const double *c2 = a.v2(), *c3 = a.v3();
+      if (stage == kInit) {
+        for (int r = lane; r < p; r += 32) a.w()[r] = 1.0;
+        __syncwarp();
+        slack = false;
+        c1 = (lane < n) ? -q + gcol_dot(a.h()) : 0.0;  // r1 = -q + G' h
+        c4 = b;
+      } else if (stage == kStep) {
+        if (it >= kMaxIters || converged) {  // the while-loop condition of qpax
+          if (op == kOpBwd) {
+            if (P->out[0]) store_iterate(R, false);
+            stage = kAdjoint;
+            continue;
+          }
+          stage = kDone;
+          continue;
+        }
+        const double nrm = residuals(relaxed ? P->kappa : 0.0, v1, v4);
+        conv_now = (nrm < P->tol) ? 1 : 0;
+        c1 = v1;
+        c4 = v4;
+      } else if (stage == kCorrector) {
+        refactor = false;
+        c1 = v1;
+        c4 = v4;
+      } else {  // kAdjoint
+        for (int r = lane; r < p; r += 32) {
+          a.w()[r] = a.z()[r] / a.s()[r];
+          a.v2()[r] = 0.0;
+        }
+        __syncwarp();
+        c1 = (lane < n) ? -P->gx[R.oq + lane] : 0.0;
+        c3 = a.v2();
+      }
+      if (refactor) factor();
+      solve(slack, c1, c2, c3, c4, dxr, dyr);
+      // ---- consume the solution
+      if (stage == kInit) {
+        x = dxr;
+        y = dyr;
+        if (p > 0) {  // z = G x - h, then the positivity shifts (qpax/pdip.py:25-33)
+          if (lane < NP) a.xs()[lane] = x;
+          __syncwarp();
+          double zmax = -INFINITY, zmin = INFINITY;
+          for (int r = lane; r < p; r += 32) {
+            const double zr = grow_dot(r, a.xs()) - a.h()[r];
+            a.z()[r] = zr;
+            zmax = nmax(zmax, zr);
+            zmin = nmin(zmin, zr);
+          }
+          const double alpha_p = wmax(zmax);
+          const double alpha_d = -wmin(zmin);
+          for (int r = lane; r < p; r += 32) {
+            const double zr = a.z()[r];
+            a.s()[r] = (alpha_p < 0) ? -zr : -zr + (1.0 + alpha_p);
+            if (alpha_d >= 0) a.z()[r] = zr + (1.0 + alpha_d);
+          }
+          __syncwarp();
+        }
+        stage = (op == kOpSolve && p > 0) ? kStep : kDone;
+        if (op == kOpSolve && p == 0) converged = 1;  // qpax/pdip.py:208-217
+      } else if (stage == kStep && !relaxed) {
+        // predictor done (ds, dz hold ds_a, dz_a): centering_params, qpax/pdip.py:76-84
+        double sz = 0.0;
+        for (int r = lane; r < p; r += 32) sz = fma(a.s()[r], a.z()[r], sz);
+        sz = wsum(sz);
+        const double mu = sz / p;
+        const double alpha_a = nmin(1.0, wmin(nmin(ls_local(a.s(), a.ds()), ls_local(a.z(), a.dz()))));
+        double num = 0.0;
+        for (int r = lane; r < p; r += 32)
+          num = fma(a.s()[r] + alpha_a * a.ds()[r], a.z()[r] + alpha_a * a.dz()[r], num);
+        num = wsum(num);
+        const double ratio = num / sz;
+        sigma_mu = ratio * ratio * ratio * mu;
+        for (int r = lane; r < p; r += 32) a.v2()[r] = -(-a.v2()[r] - (sigma_mu - a.ds()[r] * a.dz()[r]));
+        __syncwarp();
+        stage = kCorrector;
+      } else if (stage == kStep || stage == kCorrector) {
+        // step length and update (qpax/pdip.py:112-117, pdip_relaxed.py:30-35)
+        const double ls = wmin(nmin(ls_local(a.s(), a.ds()), ls_local(a.z(), a.dz())));
+        const double alpha = relaxed ? 0.99 * nmin(1.0, 0.99 * nmin(1.0, ls)) : 0.99 * nmin(1.0, ls);
+        x += alpha * dxr;
+        y += alpha * dyr;
+        for (int r = lane; r < p; r += 32) {
+          a.s()[r] += alpha * a.ds()[r];
+          a.z()[r] += alpha * a.dz()[r];
+        }
+        __syncwarp();
+        ++it;
+        converged = conv_now;
+        stage = kStep;
+      } else {  // kAdjoint
+        write_grads(R, dxr, dyr);
+        stage = kDone;
+      }
+    }
+    if (op == kOpSolve || op == kOpInit || op == kOpRelax) store_iterate(R, op == kOpSolve);
+    if (lane == 0) {
+      if (P->conv) P->conv[inst] = (op == kOpInit || op == kOpAdjoint) ? 0 : converged;
+      if (P->iters) P->iters[inst] = it;
+      if (P->stats) {
+        P->stats[inst * 4 + kStatFact32] = 0;
+        P->stats[inst * 4 + kStatFact64] = st_f64;
+        P->stats[inst * 4 + kStatSweeps] = 0;
+        P->stats[inst * 4 + kStatFlags] = st_flags;
+      }
+    }
+    __syncwarp();
+  }
+};
+
+}  // namespace qpb

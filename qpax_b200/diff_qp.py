@@ -77,6 +77,46 @@ def diff_qp(Q, q, A, b, G, h, x, s, lam, nu, dl_dx, *, precision=None, team_thre
     return bt.out(dQ, dq, dA, db, dG, dh)
 
 
+def solve_qp_primal_vjp_host(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, target_kappa: float = 1e-3, *,
+                             out=None, chunks: int = 4, streams: int = 3, precision=None):
+    """solve_qp_primal_vjp for batches that live in host memory.
+
+    Inputs are CPU tensors with a leading batch axis (pinned memory lets the
+    copies overlap); the batch is cut into `chunks`, and on `streams` CUDA
+    streams each chunk is copied in, solved forward and backward, and its x
+    and six gradients copied back while the next chunk computes.  `out` may
+    hold preallocated pinned CPU tensors (x, dQ, dq, dA, db, dG, dh).
+    Returns (x, (dQ, dq, dA, db, dG, dh)) on the host; waits for completion.
+    """
+    dev = _lib.device()
+    B = Q.shape[0]
+    if out is None:
+        pin = torch.cuda.is_available()
+        out = [torch.empty(t.shape, dtype=torch.float64, pin_memory=pin) for t in (q, Q, q, A, b, G, h)]
+    bounds = [round(i * B / chunks) for i in range(chunks + 1)]
+    pool = [torch.cuda.Stream(device=dev) for _ in range(max(1, streams))]
+    main = torch.cuda.current_stream(dev)
+    for s in pool:
+        s.wait_stream(main)
+    opts = dict(precision=precision)
+    for c in range(chunks):
+        lo, hi = bounds[c], bounds[c + 1]
+        if hi <= lo:
+            continue
+        s = pool[c % len(pool)]
+        with torch.cuda.stream(s):
+            dev_in = [t[lo:hi].to(dev, non_blocking=True) for t in (Q, q, A, b, G, h, dl_dx)]
+            x, grads, _, _ = solve_qp_primal_vjp(*dev_in[:6], dev_in[6], solver_tol, target_kappa, **opts)
+            for dst, src in zip(out, (x,) + tuple(grads)):
+                dst[lo:hi].copy_(src, non_blocking=True)
+            for t in dev_in:
+                t.record_stream(s)
+    for s in pool:
+        main.wait_stream(s)
+    torch.cuda.synchronize(dev)
+    return out[0], tuple(out[1:])
+
+
 def solve_qp_primal_vjp(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, target_kappa: float = 1e-3, *,
                         precision=None, team_threads=None):
     """Forward and backward of solve_qp_primal as two launches, without autograd.

@@ -1,0 +1,139 @@
+"""Uneven batches: instances of different (n, m, p) in one call.
+
+qpax runs one jit(vmap(solve_qp)) per distinct shape (its early exits branch
+on Python shapes, qpax/pdip.py:208-217).  Here a plan groups the instances by
+kernel variant once; each call then launches one persistent kernel per size
+bin, concurrently, from the caller's stream (capturable in a CUDA graph).
+
+    plan = PackedPlan(shapes)                     # [(n, m, p), ...], p >= 1
+    x, s, z, y, conv, iters = plan.solve(Q, q, A, b, G, h, solver_tol)   # packed 1-D tensors
+    dQ, dq, dA, db, dG, dh = plan.primal_bwd(Q, ..., x, s, z, y, dl_dx, solver_tol, kappa)
+
+Packed layout: each array is the concatenation of the per-instance row-major
+arrays in instance order.  `pack` / `unpack` convert from / to lists.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_SIGS = {
+    "qpb_plan_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_void_p,
+                         ctypes.POINTER(_lib.Config)], ctypes.c_int),
+    "qpb_plan_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "qpb_plan_workspace_size": ([ctypes.c_void_p], ctypes.c_size_t),
+    "qpb_plan_num_bins": ([ctypes.c_void_p], ctypes.c_int32),
+    "qpb_plan_totals": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "qpb_solve_qp_packed": ([ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_double] + [ctypes.c_void_p] * 6 +
+                            [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p], ctypes.c_int),
+    "qpb_solve_qp_primal_bwd_packed": ([ctypes.c_void_p] + [ctypes.c_void_p] * 11 + [ctypes.c_double] * 2 +
+                                       [ctypes.c_void_p] * 6 + [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+                                       ctypes.c_int),
+}
+
+
+def _load():
+    lib = _lib.load()
+    if not getattr(lib, "_qpb_packed_ready", False):
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        lib._qpb_packed_ready = True
+    return lib
+
+
+def sizes(shapes):
+    """Per-instance lengths of (Q, q, A, b, G, h)."""
+    sh = np.asarray(shapes, dtype=np.int64).reshape(-1, 3)
+    n, m, p = sh[:, 0], sh[:, 1], sh[:, 2]
+    return [n * n, n, m * n, m, p * n, p]
+
+
+def pack(arrays, device=None) -> torch.Tensor:
+    """Concatenate per-instance arrays (any shapes) into one 1-D float64 tensor."""
+    dev = device or _lib.device()
+    parts = [torch.as_tensor(a, dtype=torch.float64).reshape(-1) for a in arrays]
+    return torch.cat(parts).to(dev) if parts else torch.zeros(0, dtype=torch.float64, device=dev)
+
+
+def unpack(t: torch.Tensor, lengths, shapes=None):
+    """Split a packed tensor back into per-instance pieces (reshaped when shapes given)."""
+    out = list(torch.split(t, [int(v) for v in lengths]))
+    if shapes is not None:
+        out = [o.reshape(s) for o, s in zip(out, shapes)]
+    return out
+
+
+class PackedPlan:
+    """A plan for one uneven batch (shapes fixed at construction)."""
+
+    def __init__(self, shapes, precision: str = "auto", team_threads: int = 0):
+        self.lib = _load()
+        self.dev = _lib.device()
+        self.shapes = np.ascontiguousarray(np.asarray(shapes, dtype=np.int32).reshape(-1, 3))
+        self.batch = int(self.shapes.shape[0])
+        self.cfg = _lib.make_config(precision, team_threads)
+        h = ctypes.c_void_p()
+        st = self.lib.qpb_plan_create(ctypes.byref(h), self.batch, self.shapes.ctypes.data, ctypes.byref(self.cfg))
+        if st != 0:
+            raise _lib.QpbError(f"qpb_plan_create: {self.lib.qpb_status_string(st).decode()} (status {st})")
+        self.handle = h
+        tot = (ctypes.c_int64 * 6)()
+        self.lib.qpb_plan_totals(self.handle, ctypes.addressof(tot))
+        self.totals = [int(v) for v in tot]
+        self.num_bins = int(self.lib.qpb_plan_num_bins(self.handle))
+        nbytes = int(self.lib.qpb_plan_workspace_size(self.handle))
+        self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.dev)
+        self.lengths = sizes(self.shapes)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self.lib.qpb_plan_destroy(h)
+            self.handle = None
+
+    def _ws(self):
+        return _lib.aligned(self.workspace)
+
+    def new(self, k, dtype=torch.float64):
+        return torch.empty(self.totals[k], dtype=dtype, device=self.dev)
+
+    def solve(self, Q, q, A, b, G, h, solver_tol: float = 1e-3):
+        """qpb_solve_qp_packed -> packed (x, s, z, y) and per-instance (converged, iters)."""
+        x, s, z, y = self.new(1), self.new(5), self.new(5), self.new(3)
+        conv = torch.empty(self.batch, dtype=torch.int32, device=self.dev)
+        iters = torch.empty(self.batch, dtype=torch.int32, device=self.dev)
+        wp, wb = self._ws()
+        _lib.call("qpb_solve_qp_packed", self.handle, *[_lib.ptr(t) for t in (Q, q, A, b, G, h)],
+                  ctypes.c_double(solver_tol), *[_lib.ptr(t) for t in (x, s, z, y, conv, iters)], wp, wb,
+                  _lib.stream_handle())
+        return x, s, z, y, conv, iters
+
+    def primal_bwd(self, Q, q, A, b, G, h, x, s, z, y, dl_dx, solver_tol: float = 1e-5,
+                   target_kappa: float = 1e-3):
+        """qpb_solve_qp_primal_bwd_packed -> packed (dQ, dq, dA, db, dG, dh)."""
+        grads = [self.new(k) for k in range(6)]
+        wp, wb = self._ws()
+        _lib.call("qpb_solve_qp_primal_bwd_packed", self.handle,
+                  *[_lib.ptr(t) for t in (Q, q, A, b, G, h, x, s, z, y, dl_dx)], ctypes.c_double(solver_tol),
+                  ctypes.c_double(target_kappa), *[_lib.ptr(t) for t in grads], wp, wb, _lib.stream_handle())
+        return tuple(grads)
+
+
+def solve_qp_uneven(Qs, qs, As, bs, Gs, hs, solver_tol: float = 1e-3, precision: str = "auto"):
+    """solve_qp over lists of per-instance arrays of different shapes.
+
+    Returns lists (x_i), (s_i), (z_i), (y_i) and tensors (converged, iters).
+    """
+    shapes = [(np.shape(Q)[0], np.shape(b)[0], np.shape(h)[0]) for Q, b, h in zip(Qs, bs, hs)]
+    plan = PackedPlan(shapes, precision)
+    ins = [pack(v, plan.dev) for v in (Qs, qs, As, bs, Gs, hs)]
+    x, s, z, y, conv, iters = plan.solve(*ins, solver_tol)
+    L = plan.lengths
+    return unpack(x, L[1]), unpack(s, L[5]), unpack(z, L[5]), unpack(y, L[3]), conv, iters
