@@ -201,13 +201,21 @@ def run_reference(args, world, rank):
 
 
 def load_traffic():
-    path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(path):
-        try:
-            return json.load(open(path))
-        except ValueError:
-            return None
-    return None
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+    bench workload's forward and backward launches, from the committed ncu
+    summary profiles/traffic_dense_qp_n32_b4096.txt ("key value" lines)."""
+    path = os.path.join(ROOT, "profiles", "traffic_dense_qp_n32_b4096.txt")
+    if not os.path.exists(path):
+        return None
+    out = {"source": "profiles/traffic_dense_qp_n32_b4096.txt"}
+    for ln in open(path):
+        parts = ln.split()
+        if len(parts) == 2 and parts[0] in ("forward", "backward"):
+            try:
+                out[parts[0]] = float(parts[1])
+            except ValueError:
+                pass
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -227,8 +235,7 @@ def run_ours(args, world, rank, local):
     dl_host = np.full((B, N), 0.1)
     stream = torch.cuda.current_stream()
 
-    def make_step(prec):
-        opts = dict(precision=prec)
+    def make_step(opts):
         cfg = _config(opts)
         x, s, z, y = bt.new(B, N), bt.new(B, P), bt.new(B, P), bt.new(B, M)
         conv, iters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
@@ -262,15 +269,22 @@ def run_ours(args, world, rank, local):
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     results = {}
-    for prec in (["fp64", "mixed"] if not args.only_mixed else ["mixed"]):
-        step, outs = make_step(prec)
+    variants = {
+        "auto": dict(precision="auto"),                       # the default path (warp kernel here)
+        "fp64_cta": dict(precision="fp64", team_threads=128),  # plain FP64, one QP per CTA
+        "mixed": dict(precision="mixed"),                     # FP32 factor + FP64 refinement
+    }
+    if args.only_default:
+        variants = {"auto": variants["auto"]}
+    for prec, opts in variants.items():
+        step, outs = make_step(opts)
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
         barrier(world)
         torch.cuda.synchronize()
-        sampler = ClockSampler(local) if prec == "mixed" else None
+        sampler = ClockSampler(local) if prec == "auto" else None
         if sampler:
             sampler.__enter__()
         wall0 = time.perf_counter()
@@ -292,50 +306,58 @@ def run_ours(args, world, rank, local):
                              riters=riters.cpu().numpy(), rconv=rconv.cpu().numpy(),
                              clocks=sampler.summary() if sampler else None)
 
-    mixed = results["mixed"]
-    value = world * B * args.steps / (mixed["total_ms"] * 1e-3)
-    # roofline of the dominant launch (forward or backward kernel)
-    f_fwd, f_bwd = algorithmic_flops(N, M, P, mixed["iters"].astype(np.float64), mixed["riters"].astype(np.float64))
+    main_r = results["auto"]
+    value = world * B * args.steps / (main_r["total_ms"] * 1e-3)
+    # roofline of the dominant launch (forward or backward kernel of the default path)
+    f_fwd, f_bwd = algorithmic_flops(N, M, P, main_r["iters"].astype(np.float64),
+                                     main_r["riters"].astype(np.float64))
     fl_fwd, fl_bwd = float(f_fwd.sum()), float(f_bwd.sum())
-    if mixed["fwd_ms"] >= mixed["bwd_ms"]:
-        dom, dom_ms, dom_fl = "qpb_solve_qp (ipm_kernel<StdQP<128,1,mixed>>)", mixed["fwd_ms"], fl_fwd
+    traffic = load_traffic()
+    if main_r["fwd_ms"] >= main_r["bwd_ms"]:
+        dom, dom_ms, dom_fl, dom_key = "qpb_solve_qp: warp_kernel<32,8> (forward)", main_r["fwd_ms"], fl_fwd, "forward"
     else:
-        dom, dom_ms, dom_fl = "qpb_solve_qp_primal_bwd (ipm_kernel<StdQP<128,1,mixed>>)", mixed["bwd_ms"], fl_bwd
+        dom, dom_ms, dom_fl, dom_key = "qpb_solve_qp_primal_bwd: warp_kernel<32,8> (backward)", main_r["bwd_ms"], \
+            fl_bwd, "backward"
     achieved = dom_fl / (dom_ms * 1e-3) / 1e12
     peaks, peak_src = load_peaks()
     simt = simt_peaks()
-    traffic = load_traffic()
     roof = {
         "bound": "tensor", "kernel": dom, "achieved": achieved, "unit": "TFLOP/s",
-        "peak": simt["fp32_tflops"], "frac": achieved / simt["fp32_tflops"],
-        "peak_source": f"FP32 SIMT FMA peak measured in this run ({simt['how']}); the kernel is FP32/FP64 "
-                       "SIMT arithmetic, not tensor-core work",
-        "frac_of_fp64_simt_peak": achieved / simt["fp64_tflops"], "fp64_simt_peak": simt["fp64_tflops"],
-        "frac_of_bf16_tensor_peak": achieved / peaks["bf16_tflops"], "bf16_peak_source": peak_src,
-        "algorithmic_flops_per_launch": dom_fl,
-        "traffic": (traffic or {}).get("bytes_per_launch"),
+        "peak": peaks["bf16_tflops"], "frac": achieved / peaks["bf16_tflops"],
+        "peak_source": f"bf16 dense tensor peak of MEASURED_PEAKS.json ({peak_src}); the kernel is FP64 "
+                       "arithmetic, so its own roof is the FP64 FMA peak below",
+        "fp64_fma_peak": simt["fp64_tflops"], "frac_of_fp64_fma_peak": achieved / simt["fp64_tflops"],
+        "fp32_fma_peak": simt["fp32_tflops"], "fma_peak_source": simt["how"],
+        "algorithmic_flops_per_launch": dom_fl, "avg_launch_ms": dom_ms,
+        "traffic": (traffic or {}).get(dom_key),
+        "traffic_source": (traffic or {}).get("source"),
     }
     line = {
         "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": mixed["total_ms"] / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": main_r["total_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "global_batch": B * world, "n": N, "m": M, "p": P,
-                   "precision": "mixed (FP32 factor + FP64 refinement)", "parallelism": f"batch split x{world}",
+                   "precision": "auto (FP64; one warp per QP for n <= 32)", "parallelism": f"batch split x{world}",
                    "l2": "flushed between steps (256 MB write), outside the per-step events"},
-        "fp64_plain": None, "mixed_over_fp64": None,
         "roofline": roof, "gpu_launches": 2 * args.steps,
-        "iterations": {"forward_mean": float(mixed["iters"].mean()), "relax_mean": float(mixed["riters"].mean()),
-                       "converged": float(mixed["conv"].mean())},
-        "clocks": mixed["clocks"],
+        "iterations": {"forward_mean": float(main_r["iters"].mean()), "relax_mean": float(main_r["riters"].mean()),
+                       "converged": float(main_r["conv"].mean())},
+        "clocks": main_r["clocks"],
+        "forward_ms": main_r["fwd_ms"], "backward_ms": main_r["bwd_ms"],
     }
-    if "fp64" in results:
-        f = results["fp64"]
-        v64 = world * B * args.steps / (f["total_ms"] * 1e-3)
-        line["fp64_plain"] = {"value": v64, "unit": "QPs/s", "ms_per_step": f["total_ms"] / args.steps,
-                              "kernel": "same IPM, FP64 factor, one QP per 128-thread CTA"}
-        line["mixed_over_fp64"] = value / v64
-        line["converged_flags_identical"] = bool((f["conv"] == mixed["conv"]).all())
-        line["iteration_counts_identical"] = bool((f["iters"] == mixed["iters"]).all())
+    if "fp64_cta" in results and "mixed" in results:
+        v = {k: world * B * args.steps / (r["total_ms"] * 1e-3) for k, r in results.items()}
+        line["variants"] = {
+            "fp64_one_cta_per_qp": {"value": v["fp64_cta"], "unit": "QPs/s",
+                                    "ms_per_step": results["fp64_cta"]["total_ms"] / args.steps},
+            "mixed_fp32_factor_fp64_refinement": {"value": v["mixed"], "unit": "QPs/s",
+                                                  "ms_per_step": results["mixed"]["total_ms"] / args.steps},
+        }
+        line["mixed_over_plain_fp64"] = v["mixed"] / v["fp64_cta"]
+        line["default_over_plain_fp64"] = v["auto"] / v["fp64_cta"]
+        line["converged_flags_identical"] = bool(all((r["conv"] == main_r["conv"]).all() for r in results.values()))
+        line["iteration_counts_identical"] = bool(all((r["iters"] == main_r["iters"]).all()
+                                                      for r in results.values()))
     if rank == 0 and not args.no_e2e:
         line["e2e"] = run_e2e(args, data, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -387,11 +409,7 @@ def run_e2e(args, data, dev):
     d2h = sum(t.numel() * 8 for t in outs_host)
 
     def step():
-        dev_in = [t.to(dev, non_blocking=True) for t in host]
-        g = g_host.to(dev, non_blocking=True)
-        x, grads, _, _ = qb.solve_qp_primal_vjp(*dev_in, g, TOL, KAPPA)
-        for dst, src in zip(outs_host, (x,) + tuple(grads)):
-            dst.copy_(src, non_blocking=True)
+        qb.solve_qp_primal_vjp_host(*host, g_host, TOL, KAPPA, out=outs_host, chunks=args.e2e_chunks)
 
     for _ in range(args.warmup):
         step()
@@ -405,7 +423,8 @@ def run_e2e(args, data, dev):
     ms = e0.elapsed_time(e1)
     return {"value": B * args.steps / (ms * 1e-3), "unit": "QPs/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps,
-            "path": "qpax_b200.solve_qp_primal_vjp (C ABI) from pinned host tensors"}
+            "path": f"qpax_b200.solve_qp_primal_vjp_host (C ABI): pinned host tensors, {args.e2e_chunks} chunks "
+                    "pipelined over 3 streams (copy in / solve + backward / copy out overlap)"}
 
 
 def main():
@@ -414,7 +433,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--only-mixed", action="store_true")
+    ap.add_argument("--only-default", action="store_true", help="time only the default (auto) path")
+    ap.add_argument("--e2e-chunks", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

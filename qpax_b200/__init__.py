@@ -12,7 +12,7 @@ Arrays take a leading batch axis where qpax users would jax.vmap.  Compute
 runs in libqpb.so (include/qpb.h); there is no CPU path.
 """
 
-from .diff_qp import diff_qp, solve_qp_primal, solve_qp_primal_vjp
+from .diff_qp import diff_qp, solve_qp_primal, solve_qp_primal_vjp, solve_qp_primal_vjp_host
 from .elastic_qp import (diff_qp_elastic, initialize_elastic, relax_qp_elastic, solve_qp_elastic,
                          solve_qp_elastic_primal, solve_qp_elastic_primal_vjp)
 from .pdip import initialize, relax_qp, set_defaults, solve_qp

@@ -52,6 +52,60 @@ static DevInfo dev_info() {
   return cache[dev];
 }
 
+// Per (device, kernel, block, shared memory): raises the kernel's dynamic
+// shared-memory limit once and caches its occupancy, so planning a launch
+// makes no CUDA call after the first time (those calls can serialize work
+// in flight on other streams).
+struct OccKey {
+  int dev;
+  const void* fn;
+  int threads;
+  size_t smem;
+};
+static int occupancy(const void* fn, int threads, size_t smem, int* per_sm) {
+  static std::mutex mu;
+  static OccKey keys[256];
+  static int vals[256];
+  static int count = 0;
+  // per (device, kernel): the dynamic shared-memory limit set so far.  The
+  // limit only ever grows, so every earlier plan of the kernel stays valid.
+  static OccKey limits[128];
+  static int nlimits = 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return QPB_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(mu);
+  for (int i = 0; i < count; ++i)
+    if (keys[i].dev == dev && keys[i].fn == fn && keys[i].threads == threads && keys[i].smem == smem) {
+      *per_sm = vals[i];
+      return QPB_OK;
+    }
+  if (smem > 48 * 1024) {
+    int li = -1;
+    for (int i = 0; i < nlimits; ++i)
+      if (limits[i].dev == dev && limits[i].fn == fn) li = i;
+    if (li < 0 || limits[li].smem < smem) {
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return QPB_ERR_CUDA;
+      if (li >= 0) {
+        limits[li].smem = smem;
+      } else if (nlimits < 128) {
+        limits[nlimits++] = OccKey{dev, fn, 0, smem};
+      } else {
+        return QPB_ERR_CUDA;
+      }
+    }
+  }
+  int v = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, fn, threads, smem) != cudaSuccess) return QPB_ERR_CUDA;
+  if (count < 256) {
+    keys[count] = OccKey{dev, fn, threads, smem};
+    vals[count] = v;
+    ++count;
+  }
+  *per_sm = v;
+  return QPB_OK;
+}
+
 // Padded column count of the one-warp-per-instance kernel, or 0 when the
 // instance does not fit it (n <= 32, m <= NP / 4).
 int warp_np(const qpb_dims& d) {
@@ -83,14 +137,8 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
       pl->in_smem = 0;
       pl->smem_bytes = 0;
     }
-    if (pl->smem_bytes > 48 * 1024 &&
-        cudaFuncSetAttribute(pl->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem_bytes) !=
-            cudaSuccess)
-      return QPB_ERR_CUDA;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->fn, pl->threads, pl->smem_bytes) !=
-        cudaSuccess)
-      return QPB_ERR_CUDA;
+    if (occupancy(pl->fn, pl->threads, pl->smem_bytes, &per_sm) != QPB_OK) return QPB_ERR_CUDA;
     if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
     if (!pl->in_smem && per_sm > 4) per_sm = 4;
     const long need = ((long)d.batch + pl->teams - 1) / pl->teams;
@@ -128,14 +176,8 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     pl->smem_bytes = 0;
   }
   pl->threads = NT * pl->teams;
-  if (pl->smem_bytes > 48 * 1024) {
-    if (cudaFuncSetAttribute(pl->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem_bytes) !=
-        cudaSuccess)
-      return QPB_ERR_CUDA;
-  }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->fn, pl->threads, pl->smem_bytes) != cudaSuccess)
-    return QPB_ERR_CUDA;
+  if (occupancy(pl->fn, pl->threads, pl->smem_bytes, &per_sm) != QPB_OK) return QPB_ERR_CUDA;
   if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
   if (!pl->in_smem && per_sm > 2) per_sm = 2;
   const long need = ((long)d.batch + pl->teams - 1) / pl->teams;

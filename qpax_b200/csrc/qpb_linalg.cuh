@@ -115,6 +115,45 @@ QPB_NOINLINE void form_H(const Team<NT>& t, int n, int p, const double* Q, int l
   }
 }
 
+// Lower triangle of H = sym(Q) + G' diag(w) G in FP64 on the tensor cores:
+// 8x8 tiles of H, one warp per tile, accumulated over p in steps of 4 with
+// mma.m8n8k4.f64 (fragments: a0 = A[lane/4][lane%4], b0 = B[lane%4][lane/4],
+// (d0, d1) = D[lane/4][2*(lane%4) + {0,1}]).  Columns beyond n read as zero.
+template <int NT>
+QPB_NOINLINE void form_H_dmma(const Team<NT>& t, int n, int p, const double* Q, int ldq, const double* G, int ldg,
+                              const double* wv, double* H, int ldh) {
+  const int nb = (n + 7) >> 3;
+  const int ntiles = nb * (nb + 1) / 2;
+  const int lane = t.lane(), g = lane >> 2, tg = lane & 3;
+  for (int tau = t.warp(); tau < ntiles; tau += NT / 32) {
+    int bi = (int)((sqrtf(8.0f * tau + 1.0f) - 1.0f) * 0.5f);
+    while (bi * (bi + 1) / 2 > tau) --bi;
+    while ((bi + 1) * (bi + 2) / 2 <= tau) ++bi;
+    const int bj = tau - bi * (bi + 1) / 2;
+    const int ci = 8 * bi + g, cj = 8 * bj + g;  // A row / B column this lane feeds
+    double d0 = 0.0, d1 = 0.0;
+    for (int k0 = 0; k0 < p; k0 += 4) {
+      const int k = k0 + tg;
+      const bool in = k < p;
+      const double* row = G + (size_t)(in ? k : 0) * ldg;
+      const double a0 = (in && ci < n) ? wv[k] * row[ci] : 0.0;
+      const double b0 = (in && cj < n) ? row[cj] : 0.0;
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                   : "+d"(d0), "+d"(d1)
+                   : "d"(a0), "d"(b0));
+    }
+    const int i = 8 * bi + g;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int j = 8 * bj + 2 * tg + e;
+      if (i < n && j <= i) {
+        const double qs = 0.5 * (Q[(size_t)i * ldq + j] + Q[(size_t)j * ldq + i]);
+        H[(size_t)i * ldh + j] = qs + (e ? d1 : d0);
+      }
+    }
+  }
+}
+
 // Factor the reduced KKT matrix for weights wv.  G, A are n4-padded FP64.
 // For R == float, GS (p x ldg floats) is scratch for sqrt(w)-scaled G.
 // Returns the H pivot ratio (+inf when the factor is unusable) to all threads.
@@ -129,7 +168,7 @@ QPB_NOINLINE double factor_kkt(const Team<NT>& t, int n, int m, int p, const dou
     t.sync();
     form_H<NT, float, float, false>(t, n, p, Q, ld, GS, ld, wv, f.L, f.ldl);
   } else {
-    form_H<NT, double, double, true>(t, n, p, Q, ld, G, ld, wv, f.L, f.ldl);
+    form_H_dmma<NT>(t, n, p, Q, ld, G, ld, wv, f.L, f.ldl);
   }
   t.sync();
   const double ratio = ldlt<NT, R>(t, n, f.L, f.ldl, f.dinv);

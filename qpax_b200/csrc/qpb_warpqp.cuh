@@ -47,7 +47,8 @@ QPB_DEV double wmin(double v) {
 // Addresses are recomputed from the base and p where used (no pointer table).
 struct WarpArena {
   static __host__ __device__ size_t doubles(int NP, int MP, int p) {
-    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + 3 * (size_t)NP + (size_t)MP * NP +
+    // the Y region doubles as the 8 x NP tile-row scratch of the H formation
+    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + 3 * (size_t)NP + (size_t)(MP > 8 ? MP : 8) * NP +
            (size_t)MP * MP;
   }
   static size_t bytes(int NP, int MP, int p) { return doubles(NP, MP, p) * sizeof(double) + 16; }
@@ -75,7 +76,7 @@ struct WarpAddr {
   QPB_DEV double* cb() const { return xs() + NP; }
   QPB_DEV double* dvi() const { return xs() + 2 * NP; }
   QPB_DEV double* Y() const { return xs() + 3 * NP; }
-  QPB_DEV double* F() const { return Y() + MP * NP; }
+  QPB_DEV double* F() const { return Y() + (MP > 8 ? MP : 8) * NP; }
 };
 
 template <int NP, int MP>
@@ -100,10 +101,14 @@ struct WarpQP {
     a.p = p;
   }
 
-  // sym(Q)[i][lane] through L1 (Q is symmetrized on the fly: (Q + Q')/2).
+  // sym(Q)[i][lane] through L1: (Q + Q')/2, or the coalesced Q[i][lane]
+  // alone when Q is exactly symmetric (checked once per instance).
   QPB_DEV double qsym(int i) const {
-    return (i < n && lane < n) ? 0.5 * (gQ[i * n + lane] + gQ[lane * n + i]) : 0.0;
+    if (!(i < n && lane < n)) return 0.0;
+    const double v = gQ[i * n + lane];
+    return q_symmetric ? v : 0.5 * (v + gQ[lane * n + i]);
   }
+  bool q_symmetric;
 
   QPB_DEV void load(const InstRef& R, bool remove_inf) {
     gQ = P->Q + R.oQ;
@@ -124,6 +129,10 @@ struct WarpQP {
     }
     q = (lane < n) ? P->q[R.oq + lane] : 0.0;
     b = (lane < m) ? P->b[R.ob + lane] : 0.0;
+    int asym = 0;
+    if (lane < n)
+      for (int i = 0; i < n; ++i) asym |= (gQ[i * n + lane] != gQ[lane * n + i]);
+    q_symmetric = !__any_sync(kFull, asym);
     __syncwarp();
   }
 
@@ -151,6 +160,77 @@ struct WarpQP {
     }
   }
 
+  // -------------------------------------------------- G' diag(w) G on DMMA
+  // D (8x8) += A (8x4, row) * B (4x8, col) in FP64 on the tensor cores.
+  // Fragments (PTX mma.m8n8k4 .f64): a0 = A[lane/4][lane%4],
+  // b0 = B[lane%4][lane/4], (d0, d1) = D[lane/4][2*(lane%4) + {0, 1}].
+  static QPB_DEV void dmma884(double& d0, double& d1, double a0, double b0) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a0), "d"(b0));
+  }
+
+  // hc[i] = (G' diag(w) G)[i][lane].  The lower-triangle 8x8 tiles are
+  // accumulated one tile row at a time on the FP64 tensor cores
+  // (H_tile(ti, tj) = sum_k (w_k G[k][8ti..]) (x) G[k][8tj..]); each finished
+  // tile row goes through the 8 x NP scratch (the Y region, rebuilt later in
+  // factor()) into the lane-owns-a-column layout, the upper triangle coming
+  // from the symmetric element of a later tile row.
+  template <int TI>
+  QPB_DEV void h_tile_row() {
+    const int g = lane >> 2, t = lane & 3;
+    const double* Gs = a.G();
+    const double* wv = a.w();
+    double* S = a.Y();
+    const int kblocks = (p + 3) >> 2;
+    double acc[TI + 1][2];
+#pragma unroll
+    for (int tj = 0; tj <= TI; ++tj) acc[tj][0] = acc[tj][1] = 0.0;
+    for (int kb = 0; kb < kblocks; ++kb) {
+      const int k = 4 * kb + t;
+      const bool in = k < p;
+      const double* row = Gs + (in ? k : 0) * NP;
+      const double a0 = in ? wv[k] * row[8 * TI + g] : 0.0;  // (diag(w) G)'[8TI+g][k]
+#pragma unroll
+      for (int tj = 0; tj <= TI; ++tj) {
+        const double b0 = in ? row[8 * tj + g] : 0.0;  // G[k][8tj+g]
+        dmma884(acc[tj][0], acc[tj][1], a0, b0);
+      }
+    }
+#pragma unroll
+    for (int tj = 0; tj <= TI; ++tj) {
+      S[g * NP + 8 * tj + 2 * t] = acc[tj][0];
+      S[g * NP + 8 * tj + 2 * t + 1] = acc[tj][1];
+    }
+    __syncwarp();
+    // Every element is taken from the lower triangle (row >= column) so that
+    // H is exactly symmetric; the factorization relies on that.
+    const int tl = lane >> 3;  // this lane's tile column
+    if (lane < NP && tl < TI) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) hc[8 * TI + r] = S[r * NP + lane];  // rows of tile row TI
+    }
+    if (lane < NP && tl == TI) {
+      const int c = lane - 8 * TI;  // column within the diagonal tile
+#pragma unroll
+      for (int r = 0; r < 8; ++r) hc[8 * TI + r] = (r >= c) ? S[r * NP + lane] : S[c * NP + 8 * TI + r];
+#pragma unroll
+      for (int i = 0; i < 8 * TI; ++i) hc[i] = S[c * NP + i];  // H[i][j] = H[j][i], i < 8TI
+    }
+    __syncwarp();
+  }
+
+  QPB_DEV void form_h_tensor() {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) hc[i] = 0.0;
+    h_tile_row<0>();
+    if constexpr (NP > 8) h_tile_row<1>();
+    if constexpr (NP > 16) {
+      h_tile_row<2>();
+      h_tile_row<3>();
+    }
+  }
+
   // ---------------------------------------------------------------- factor
   // H = sym(Q) + G' diag(w) G (w in shared memory), LDL^T in registers,
   // then Y = L^-1 A' and F = Y D^-1 Y' with its LDL^T in shared memory.
@@ -158,20 +238,9 @@ struct WarpQP {
     st_f64++;
     dinv = 0.0;
     fdinv = 0.0;
+    form_h_tensor();
 #pragma unroll
-    for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qsym(i);
-    const double* Gc = a.G() + (lane < NP ? lane : 0);
-    const double* wv = a.w();
-    for (int r = 0; r < p; ++r) {
-      const double* row = a.G() + r * NP;
-      const double ar = (lane < NP) ? wv[r] * Gc[r * NP] : 0.0;
-#pragma unroll
-      for (int i = 0; i < NP; i += 2) {
-        const double2 g2 = *reinterpret_cast<const double2*>(row + i);
-        hc[i] = fma(g2.x, ar, hc[i]);
-        hc[i + 1] = fma(g2.y, ar, hc[i + 1]);
-      }
-    }
+    for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qsym(i) + hc[i];
     // LDL^T: step k broadcasts row k of the Schur complement (= column k)
     int bad = 0;
     double* cb = a.cb();
@@ -183,10 +252,13 @@ struct WarpQP {
       const double rk = 1.0 / dk;
       if (k < n) bad |= !(dk > 0.0) || !isfinite(dk);
       if (lane == k) dinv = rk;
-      const double f = hc[k] * rk;
+      // S[i][j] -= (S[k][i] * S[k][j]) / d_k: the product is formed the same
+      // way for (i, j) and (j, i), so both triangles stay bit-identical and the
+      // row-held and column-held copies of L agree exactly.
+      const double hk = hc[k];
       if (lane > k) {
 #pragma unroll
-        for (int i = k + 1; i < NP; ++i) hc[i] = fma(-cb[i], f, hc[i]);
+        for (int i = k + 1; i < NP; ++i) hc[i] = fma(-(cb[i] * hk), rk, hc[i]);
       }
       __syncwarp();
     }

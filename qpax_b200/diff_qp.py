@@ -77,6 +77,18 @@ def diff_qp(Q, q, A, b, G, h, x, s, lam, nu, dl_dx, *, precision=None, team_thre
     return bt.out(dQ, dq, dA, db, dG, dh)
 
 
+_STREAMS: dict = {}
+
+
+def _host_streams(dev, count):
+    """Streams of the host pipeline, created once per device and reused (new
+    streams per call would defeat the caching allocator's per-stream reuse)."""
+    key = (dev.index, count)
+    if key not in _STREAMS:
+        _STREAMS[key] = [torch.cuda.Stream(device=dev) for _ in range(count)]
+    return _STREAMS[key]
+
+
 def solve_qp_primal_vjp_host(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, target_kappa: float = 1e-3, *,
                              out=None, chunks: int = 4, streams: int = 3, precision=None):
     """solve_qp_primal_vjp for batches that live in host memory.
@@ -94,7 +106,7 @@ def solve_qp_primal_vjp_host(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, 
         pin = torch.cuda.is_available()
         out = [torch.empty(t.shape, dtype=torch.float64, pin_memory=pin) for t in (q, Q, q, A, b, G, h)]
     bounds = [round(i * B / chunks) for i in range(chunks + 1)]
-    pool = [torch.cuda.Stream(device=dev) for _ in range(max(1, streams))]
+    pool = _host_streams(dev, max(1, streams))
     main = torch.cuda.current_stream(dev)
     for s in pool:
         s.wait_stream(main)
