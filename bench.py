@@ -1,6 +1,6 @@
 """Benchmark: QPs/sec, forward + backward, at 1e-6 KKT residual, one B200 per rank.
 
-Workload (one step): the differentiable batched solve of qpax
+Default workload (one step): the differentiable batched solve of qpax
 (solve_qp_primal) over 4096 dense QPs with n = 32, m = 8, p = 64 -- the
 dense-QP configuration (Q = M'M + 1e-3 I, strictly feasible h = G x0 + s0),
 solver_tol 1e-6, target_kappa 1e-3, loss ||x - 1||^2:
@@ -11,6 +11,15 @@ Inputs are resident in HBM; L2 is flushed (256 MB write) between steps,
 outside the per-step CUDA events.  Synthetic seeded data (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dense|nnls|small|uneven|elastic]
+
+Other workloads (same JSON line, `config.workload` names them):
+  nnls     10000 non-negative least squares QPs, n = 5, G = -I, no equalities
+  small    2048 dense QPs n = 16, m = 4, p = 32, solver_tol 1e-5
+  uneven   16384 QPs of different sizes: n ~ U{4..256}, p = 2n,
+           m ~ U{0..n/4}, one packed call (size-binned plan)
+  elastic  1024 elastic QPs (solve_qp_elastic_primal) n = 64, p = 128,
+           penalty 1e3, 30% of them infeasible
 
 --impl reference times the FP64 CPU restatement of qpax (oracle/) on the
 host cores, on the same workload -- qpax itself (JAX) is not installable
@@ -21,11 +30,13 @@ scaling, no collective on the data path); time = max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
 import sys
 import time
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -33,15 +44,72 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPs/sec fwd+bwd at 1e-6 KKT residual, mixed vs plain FP64 kernel, 1 B200"
-B, N, M, P = 4096, 32, 8, 64
-TOL, KAPPA = 1e-6, 1e-3
-WORKLOAD = "dense QP n=32 m=8 p=64, batch 4096/GPU, solve_qp_primal forward+backward, tol 1e-6, kappa 1e-3"
+KAPPA = 1e-3
+
+
+@dataclass
+class Spec:
+    key: str
+    kind: str          # "uniform" | "uneven" | "elastic"
+    batch: int
+    n: int
+    m: int
+    p: int
+    tol: float
+    workload: str
+
+
+WORKLOADS = {
+    "dense": Spec("dense", "uniform", 4096, 32, 8, 64, 1e-6,
+                  "dense QP n=32 m=8 p=64, batch 4096/GPU, solve_qp_primal forward+backward, tol 1e-6, kappa 1e-3"),
+    "nnls": Spec("nnls", "uniform", 10000, 5, 0, 5, 1e-6,
+                 "NNLS QP n=5 (Q=F'F, F 10x5), G=-I, no equalities, batch 10000/GPU, solve_qp_primal "
+                 "forward+backward, tol 1e-6, kappa 1e-3"),
+    "small": Spec("small", "uniform", 2048, 16, 4, 32, 1e-5,
+                  "dense QP n=16 m=4 p=32, batch 2048/GPU, solve_qp_primal forward+backward, tol 1e-5, kappa 1e-3"),
+    "uneven": Spec("uneven", "uneven", 16384, 256, 64, 512, 1e-6,
+                   "uneven batch of 16384 QPs/GPU, n~U{4..256}, p=2n, m~U{0..n/4}, one packed call, "
+                   "solve_qp_primal forward+backward, tol 1e-6, kappa 1e-3"),
+    "elastic": Spec("elastic", "elastic", 1024, 64, 0, 128, 1e-6,
+                    "elastic QP n=64 p=128 penalty 1e3 (30% infeasible), batch 1024/GPU, solve_qp_elastic_primal "
+                    "forward+backward, tol 1e-6, kappa 1e-3"),
+}
+
+
+def make_data(spec: Spec):
+    """Host (numpy) inputs of the workload, seeded."""
+    from qpax_b200 import workloads as wl
+
+    if spec.key == "dense":
+        return wl.config2(spec.batch)
+    if spec.key == "small":
+        return wl.config3(spec.batch)
+    if spec.key == "nnls":
+        return wl.nnls(spec.batch)
+    if spec.key == "uneven":
+        return wl.uneven(spec.batch)
+    Q, q, G, h, _ = wl.elastic(spec.batch)
+    return Q, q, G, h
+
+
+def shapes_of(spec: Spec, data):
+    """Per-instance (n, m, p) as int arrays."""
+    if spec.kind == "uneven":
+        n = np.array([len(v) for v in data[1]])
+        m = np.array([len(v) for v in data[3]])
+        p = np.array([len(v) for v in data[5]])
+        return n, m, p
+    B = spec.batch
+    return np.full(B, spec.n), np.full(B, spec.m), np.full(B, spec.p)
 
 
 def algorithmic_flops(n, m, p, iters_fwd, iters_relax):
-    """Algorithmic FLOPs (FMA = 2, symmetric-aware) of one forward + backward:
-    initialize + iters_fwd predictor-corrector iterations, iters_relax
-    relaxation iterations and the adjoint (one factor + one solve + outer products)."""
+    """Algorithmic FLOPs (FMA = 2, symmetric-aware) of one forward + backward
+    per instance: initialize + iters_fwd predictor-corrector iterations,
+    iters_relax relaxation iterations and the adjoint (one factor + one solve
+    + outer products).  Elastic QPs are counted with m = 0 (their reduced
+    system is the n x n matrix Q + G' diag(w) G over p rows)."""
+    n, m, p = (np.asarray(v, dtype=np.float64) for v in (n, m, p))
     f_fac = p * n * (n + 1) + n ** 3 / 3 + 2 * m * n * n + m * (m + 1) * n + m ** 3 / 3
     f_sol = 4 * n * n + 2 * m * m + 4 * m * n + 4 * p * n + 6 * p
     res = 2 * n * n + 4 * m * n + 4 * p * n
@@ -147,52 +215,84 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline_sample(data, seconds=12.0, max_seconds=30.0, chunk=1024):
-    """The oracle (FP64 C restatement of qpax, OpenMP over instances, all host
-    threads) on repeated chunks of the same batch until `seconds` elapse."""
+# ------------------------------------------------------------- CPU (oracle)
+
+def _oracle_chunk(spec: Spec, data, lo, hi, nthreads):
+    """The oracle's forward + backward on instances [lo, hi) of the workload."""
     from oracle import oracle
 
-    Q, q, A, b, G, h = data
-    dl = np.full((B, N), 0.1)
-    done, t0 = 0, time.perf_counter()
-    i = 0
+    if spec.kind == "uneven":
+        part = [v[lo:hi] for v in data]
+        dl = [np.full(len(q), 0.1) for q in part[1]]
+        oracle.solve_qp_primal_vjp(*part, dl, solver_tol=spec.tol, target_kappa=KAPPA, nthreads=nthreads)
+    elif spec.kind == "elastic":
+        Q, q, G, h = (a[lo:hi] for a in data)
+        dl = np.full((hi - lo, spec.n), 0.1)
+        oracle.solve_qp_elastic_primal_vjp(Q, q, G, h, np.full(hi - lo, 1e3), dl, solver_tol=spec.tol,
+                                           target_kappa=KAPPA, nthreads=nthreads)
+    else:
+        part = [a[lo:hi] for a in data]
+        dl = np.full((hi - lo, spec.n), 0.1)
+        oracle.solve_qp_primal_vjp(*part, dl, solver_tol=spec.tol, target_kappa=KAPPA, nthreads=nthreads)
+
+
+def cpu_sample(spec: Spec, data, seconds, nthreads, chunk):
+    """Oracle forward + backward on consecutive chunks of the workload (wrapping
+    around) until `seconds` elapse -> (QPs/s, QPs done, seconds)."""
+    B = spec.batch
+    done, t0, lo = 0, time.perf_counter(), 0
     while True:
-        s = slice((i * chunk) % B, (i * chunk) % B + chunk)
-        oracle.solve_qp_primal_vjp(Q[s], q[s], A[s], b[s], G[s], h[s], dl[s], solver_tol=TOL, target_kappa=KAPPA)
-        done += chunk
-        i += 1
+        hi = min(lo + chunk, B)
+        _oracle_chunk(spec, data, lo, hi, nthreads)
+        done += hi - lo
+        lo = 0 if hi == B else hi
         el = time.perf_counter() - t0
-        if el >= seconds or el >= max_seconds:
-            break
-    return {"value": done / el, "unit": "QPs/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{done} QPs of the workload (chunks of {chunk}), {el:.1f} s wall, forward+backward"}
+        if el >= seconds:
+            return done / el, done, el
 
 
-def run_reference(args, world, rank):
+def cpu_baseline(spec: Spec, data):
+    """The oracle (FP64 C restatement of qpax, OpenMP over instances) on all
+    host threads (~12 s sample) and on one thread (~4 s sample)."""
     from oracle import oracle
-    from qpax_b200 import workloads as wl
+
+    cores = oracle.num_threads()
+    chunk = {"uneven": 256, "elastic": 256}.get(spec.kind, 1024)
+    v, done, el = cpu_sample(spec, data, 12.0, 0, chunk)
+    v1, done1, el1 = cpu_sample(spec, data, 4.0, 1, 16)
+    return {"value": v, "unit": "QPs/s", "cores": cores, "kind": "port",
+            "sample": f"{done} QPs of the workload in order (chunks of {chunk}), {el:.1f} s wall, forward+backward",
+            "single_thread": {"value": v1, "unit": "QPs/s", "cores": 1,
+                              "sample": f"{done1} QPs in order, {el1:.1f} s wall"}}
+
+
+def run_reference(args, spec: Spec, world, rank):
+    from oracle import oracle
 
     if rank != 0:
         return
-    data = wl.config2(B)
-    Q, q, A, b, G, h = data
-    dl = np.full((B, N), 0.1)
-    step = lambda: oracle.solve_qp_primal_vjp(Q, q, A, b, G, h, dl, solver_tol=TOL, target_kappa=KAPPA)
+    data = make_data(spec)
+    B = spec.batch
+    # each step is a bounded sample of the workload: the whole batch when it
+    # is cheap on the host, else a fixed in-order slice of it
+    per_step = {"uneven": 512, "elastic": 1024}.get(spec.kind, B)
+    per_step = min(per_step, B)
+    step = lambda: _oracle_chunk(spec, data, 0, per_step, 0)
     for _ in range(args.warmup):
         step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step()
     el = time.perf_counter() - t0
-    val = B * args.steps / el
+    val = per_step * args.steps / el
     cores = oracle.num_threads()
     line = {
-        "impl": "reference", "metric": METRIC, "value": val, "unit": "QPs/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_for(spec), "value": val, "unit": "QPs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD + " (all host threads)", "global_batch": B, "n": N, "m": M, "p": P},
+        "config": config_for(spec, 1, extra={"workload": spec.workload + " (all host threads)"}),
         "cpu_baseline": {"value": val, "unit": "QPs/s", "cores": cores, "kind": "port",
-                         "sample": f"the full {B}-QP batch per step, {args.steps} steps"},
+                         "sample": f"the first {per_step} QPs of the batch per step, {args.steps} steps"},
         "e2e": {"value": val, "unit": "QPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "qpax (JAX) is not installable offline; the timed CPU implementation is the FP64 C "
                 "restatement of qpax in oracle/ (pinned to qpax's golden vectors and tests)",
@@ -200,14 +300,31 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def load_traffic():
+def metric_for(spec: Spec):
+    if spec.key == "dense":
+        return METRIC
+    return f"QPs/sec fwd+bwd at {spec.tol:g} KKT residual, 1 B200"
+
+
+def config_for(spec: Spec, world, extra=None):
+    cfg = {"workload": spec.workload, "global_batch": spec.batch * world}
+    if spec.kind == "uneven":
+        cfg.update({"n": "U{4..256}", "m": "U{0..n/4}", "p": "2n"})
+    else:
+        cfg.update({"n": spec.n, "m": spec.m, "p": spec.p})
+    cfg.update(extra or {})
+    return cfg
+
+
+def load_traffic(spec: Spec):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-    bench workload's forward and backward launches, from the committed ncu
-    summary profiles/traffic_dense_qp_n32_b4096.txt ("key value" lines)."""
-    path = os.path.join(ROOT, "profiles", "traffic_dense_qp_n32_b4096.txt")
-    if not os.path.exists(path):
+    workload's forward and backward launches, from a committed ncu summary
+    ("key value" lines), when one exists."""
+    name = {"dense": "traffic_dense_qp_n32_b4096.txt"}.get(spec.key)
+    path = os.path.join(ROOT, "profiles", name) if name else None
+    if not path or not os.path.exists(path):
         return None
-    out = {"source": "profiles/traffic_dense_qp_n32_b4096.txt"}
+    out = {"source": "profiles/" + name}
     for ln in open(path):
         parts = ln.split()
         if len(parts) == 2 and parts[0] in ("forward", "backward"):
@@ -218,68 +335,161 @@ def load_traffic():
     return out
 
 
-def run_ours(args, world, rank, local):
+# ------------------------------------------------------------- GPU arms
+
+class UniformArm:
+    """solve_qp forward + solve_qp_primal backward on a uniform batch, through
+    the C ABI with preallocated outputs (one launch each)."""
+
+    def __init__(self, spec: Spec, data, dev, opts):
+        import torch
+
+        from qpax_b200.pdip import StdBatch, _config
+
+        self.spec, self.opts = spec, opts
+        self.dev_in = [torch.tensor(a, device=dev) for a in data]
+        self.bt = bt = StdBatch(*self.dev_in)
+        self.cfg = _config(opts)
+        B, n, m, p = spec.batch, spec.n, spec.m, spec.p
+        self.x, self.s, self.z, self.y = bt.new(B, n), bt.new(B, p), bt.new(B, p), bt.new(B, m)
+        self.conv, self.iters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
+        self.rconv, self.riters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
+        self.gx = torch.empty(B, n, dtype=torch.float64, device=dev)
+        self.launches = 2
+
+    def fwd(self):
+        from qpax_b200.pdip import _run
+
+        _run("qpb_solve_qp", "solve", self.bt, self.cfg, [ctypes.c_double(self.spec.tol)],
+             [t.data_ptr() for t in (self.x, self.s, self.z, self.y, self.conv, self.iters)])
+
+    def bwd(self):
+        import torch
+
+        from qpax_b200.diff_qp import diff_qp_from_forward
+
+        torch.mul(self.x - 1.0, 2.0, out=self.gx)
+        diff_qp_from_forward(self.bt, self.x, self.s, self.z, self.y, self.gx, self.spec.tol, KAPPA, self.opts,
+                             relaxed=[None, None, None, None, self.rconv, self.riters])
+
+    def counts(self):
+        return self.conv.cpu().numpy(), self.iters.cpu().numpy(), self.riters.cpu().numpy()
+
+    def kernel_name(self, which):
+        return "qpb_solve_qp (forward)" if which == "forward" else "qpb_solve_qp_primal_bwd (backward)"
+
+
+class ElasticArm:
+    """solve_qp_elastic forward + solve_qp_elastic_primal backward."""
+
+    def __init__(self, spec: Spec, data, dev, opts):
+        import torch
+
+        from qpax_b200.elastic_qp import ElasticBatch
+
+        self.spec, self.opts = spec, opts
+        self.dev_in = [torch.tensor(a, device=dev) for a in data]
+        self.pen = torch.full((spec.batch,), 1e3, dtype=torch.float64, device=dev)
+        self.bt = ElasticBatch(*self.dev_in, self.pen)
+        self.gx = torch.empty(spec.batch, spec.n, dtype=torch.float64, device=dev)
+        self.out = None
+        self.launches = 2
+
+    def fwd(self):
+        import qpax_b200 as qb
+
+        self.out = qb.solve_qp_elastic(*self.dev_in, self.pen, self.spec.tol, **self.opts)
+
+    def bwd(self):
+        import torch
+
+        from qpax_b200.elastic_qp import _elastic_bwd
+
+        torch.mul(self.out[0] - 1.0, 2.0, out=self.gx)
+        _elastic_bwd(self.bt, [t.contiguous() for t in self.out[:6]], self.gx, self.spec.tol, KAPPA, self.opts)
+
+    def counts(self):
+        import qpax_b200 as qb
+
+        conv, iters = self.out[6].cpu().numpy(), self.out[7].cpu().numpy()
+        rel = qb.relax_qp_elastic(*self.dev_in, self.pen, *self.out[:6], self.spec.tol, KAPPA, **self.opts)
+        return conv, iters, rel[7].cpu().numpy()
+
+    def kernel_name(self, which):
+        return ("qpb_solve_qp_elastic (forward)" if which == "forward"
+                else "qpb_solve_qp_elastic_primal_bwd (backward)")
+
+
+class UnevenArm:
+    """Packed plan: every size bin of the batch launched concurrently."""
+
+    def __init__(self, spec: Spec, data, dev, opts):
+        import torch
+
+        from qpax_b200.packed import PackedPlan, pack
+
+        self.spec = spec
+        n, m, p = shapes_of(spec, data)
+        self.plan = PackedPlan(list(zip(n, m, p)), precision=opts.get("precision") or "auto",
+                               team_threads=opts.get("team_threads") or 0)
+        self.ins = [pack(v, dev) for v in data]
+        B = spec.batch
+        self.rconv = torch.empty(B, dtype=torch.int32, device=dev)
+        self.riters = torch.empty(B, dtype=torch.int32, device=dev)
+        self.gx = torch.empty(self.plan.totals[1], dtype=torch.float64, device=dev)
+        self.out = None
+        self.launches = 2 * self.plan.num_bins
+
+    def fwd(self):
+        self.out = self.plan.solve(*self.ins, self.spec.tol)
+
+    def bwd(self):
+        import torch
+
+        torch.mul(self.out[0] - 1.0, 2.0, out=self.gx)
+        self.plan.primal_bwd(*self.ins, *self.out[:4], self.gx, self.spec.tol, KAPPA,
+                             relax_out=(self.rconv, self.riters))
+
+    def counts(self):
+        return self.out[4].cpu().numpy(), self.out[5].cpu().numpy(), self.riters.cpu().numpy()
+
+    def kernel_name(self, which):
+        return (f"qpb_solve_qp_packed: {self.plan.num_bins} size-bin kernels, concurrent (forward)"
+                if which == "forward" else
+                f"qpb_solve_qp_primal_bwd_packed: {self.plan.num_bins} size-bin kernels, concurrent (backward)")
+
+
+ARMS = {"uniform": UniformArm, "elastic": ElasticArm, "uneven": UnevenArm}
+
+
+def variants_for(spec: Spec):
+    v = {"auto": dict(precision="auto")}
+    if spec.kind != "elastic":
+        v["fp64_cta"] = dict(precision="fp64", team_threads=128)  # plain FP64, one QP per CTA
+    v["mixed"] = dict(precision="mixed")                          # FP32 factor + FP64 refinement
+    return v
+
+
+def run_ours(args, spec: Spec, world, rank, local):
     import torch
 
-    import qpax_b200 as qb
     from qpax_b200 import _lib
-    from qpax_b200 import workloads as wl
-    from qpax_b200.diff_qp import diff_qp_from_forward
-    from qpax_b200.pdip import StdBatch, _config, _run
 
     _lib.load()
     dev = torch.device("cuda", torch.cuda.current_device())
-    data = wl.config2(B)
-    Qd, qd, Ad, bd, Gd, hd = (torch.tensor(a, device=dev) for a in data)
-    bt = StdBatch(Qd, qd, Ad, bd, Gd, hd)
-    dl_host = np.full((B, N), 0.1)
+    data = make_data(spec)
     stream = torch.cuda.current_stream()
-
-    def make_step(opts):
-        cfg = _config(opts)
-        x, s, z, y = bt.new(B, N), bt.new(B, P), bt.new(B, P), bt.new(B, M)
-        conv, iters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
-        rconv, riters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
-        gx = torch.empty(B, N, dtype=torch.float64, device=dev)
-        import ctypes
-
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-
-        def fwd():
-            _run("qpb_solve_qp", "solve", bt, cfg, [ctypes.c_double(TOL)],
-                 [x.data_ptr(), s.data_ptr(), z.data_ptr(), y.data_ptr(), conv.data_ptr(), iters.data_ptr()])
-
-        def bwd():
-            torch.mul(x - 1.0, 2.0, out=gx)
-            return diff_qp_from_forward(bt, x, s, z, y, gx, TOL, KAPPA, opts,
-                                        relaxed=[None, None, None, None, rconv, riters])
-
-        def step(timed=None):
-            if timed is not None:
-                timed[0].record(stream)
-            fwd()
-            if timed is not None:
-                timed[1].record(stream)
-            g = bwd()
-            if timed is not None:
-                timed[2].record(stream)
-            return g
-
-        return step, (x, conv, iters, rconv, riters)
-
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     results = {}
-    variants = {
-        "auto": dict(precision="auto"),                       # the default path (warp kernel here)
-        "fp64_cta": dict(precision="fp64", team_threads=128),  # plain FP64, one QP per CTA
-        "mixed": dict(precision="mixed"),                     # FP32 factor + FP64 refinement
-    }
+    variants = variants_for(spec)
     if args.only_default:
         variants = {"auto": variants["auto"]}
+    arm_main = None
     for prec, opts in variants.items():
-        step, outs = make_step(opts)
+        arm = ARMS[spec.kind](spec, data, dev, opts)
         for _ in range(args.warmup):
-            step()
+            arm.fwd()
+            arm.bwd()
         torch.cuda.synchronize()
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
         barrier(world)
@@ -287,81 +497,83 @@ def run_ours(args, world, rank, local):
         sampler = ClockSampler(local) if prec == "auto" else None
         if sampler:
             sampler.__enter__()
-        wall0 = time.perf_counter()
         for k in range(args.steps):
             flush.fill_(float(k))
-            step(evs[k])
+            evs[k][0].record(stream)
+            arm.fwd()
+            evs[k][1].record(stream)
+            arm.bwd()
+            evs[k][2].record(stream)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - wall0
         if sampler:
             sampler.__exit__(None, None, None)
         barrier(world)
         fwd_ms = [e[0].elapsed_time(e[1]) for e in evs]
         bwd_ms = [e[1].elapsed_time(e[2]) for e in evs]
-        tot = sum(f + b for f, b in zip(fwd_ms, bwd_ms))
-        tot = barrier_max(tot, world)
-        x, conv, iters, rconv, riters = outs
+        tot = barrier_max(sum(f + b for f, b in zip(fwd_ms, bwd_ms)), world)
+        conv, iters, riters = arm.counts()
         results[prec] = dict(total_ms=tot, fwd_ms=float(np.mean(fwd_ms)), bwd_ms=float(np.mean(bwd_ms)),
-                             wall_s=wall, conv=conv.cpu().numpy(), iters=iters.cpu().numpy(),
-                             riters=riters.cpu().numpy(), rconv=rconv.cpu().numpy(),
-                             clocks=sampler.summary() if sampler else None)
+                             conv=conv, iters=iters, riters=riters, clocks=sampler.summary() if sampler else None)
+        if prec == "auto":
+            arm_main = arm
+        else:
+            del arm
 
+    B = spec.batch
     main_r = results["auto"]
     value = world * B * args.steps / (main_r["total_ms"] * 1e-3)
-    # roofline of the dominant launch (forward or backward kernel of the default path)
-    f_fwd, f_bwd = algorithmic_flops(N, M, P, main_r["iters"].astype(np.float64),
-                                     main_r["riters"].astype(np.float64))
-    fl_fwd, fl_bwd = float(f_fwd.sum()), float(f_bwd.sum())
-    traffic = load_traffic()
-    if main_r["fwd_ms"] >= main_r["bwd_ms"]:
-        dom, dom_ms, dom_fl, dom_key = "qpb_solve_qp: warp_kernel<32,8> (forward)", main_r["fwd_ms"], fl_fwd, "forward"
-    else:
-        dom, dom_ms, dom_fl, dom_key = "qpb_solve_qp_primal_bwd: warp_kernel<32,8> (backward)", main_r["bwd_ms"], \
-            fl_bwd, "backward"
-    achieved = dom_fl / (dom_ms * 1e-3) / 1e12
+    n, m, p = shapes_of(spec, data)
+    f_fwd, f_bwd = algorithmic_flops(n, m, p, main_r["iters"].astype(np.float64), main_r["riters"].astype(np.float64))
+    fl = {"forward": float(f_fwd.sum()), "backward": float(f_bwd.sum())}
+    dom_key = "forward" if main_r["fwd_ms"] >= main_r["bwd_ms"] else "backward"
+    dom_ms = main_r["fwd_ms"] if dom_key == "forward" else main_r["bwd_ms"]
+    achieved = fl[dom_key] / (dom_ms * 1e-3) / 1e12
     peaks, peak_src = load_peaks()
     simt = simt_peaks()
+    traffic = load_traffic(spec)
     roof = {
-        "bound": "tensor", "kernel": dom, "achieved": achieved, "unit": "TFLOP/s",
+        "bound": "tensor", "kernel": arm_main.kernel_name(dom_key), "achieved": achieved, "unit": "TFLOP/s",
         "peak": peaks["bf16_tflops"], "frac": achieved / peaks["bf16_tflops"],
         "peak_source": f"bf16 dense tensor peak of MEASURED_PEAKS.json ({peak_src}); the kernel is FP64 "
                        "arithmetic, so its own roof is the FP64 FMA peak below",
         "fp64_fma_peak": simt["fp64_tflops"], "frac_of_fp64_fma_peak": achieved / simt["fp64_tflops"],
         "fp32_fma_peak": simt["fp32_tflops"], "fma_peak_source": simt["how"],
-        "algorithmic_flops_per_launch": dom_fl, "avg_launch_ms": dom_ms,
+        "algorithmic_flops_per_launch": fl[dom_key], "avg_launch_ms": dom_ms,
         "traffic": (traffic or {}).get(dom_key),
         "traffic_source": (traffic or {}).get("source"),
     }
+    prec_desc = {"uniform": "auto (FP64; one warp per QP for n <= 32, one CTA per QP above)",
+                 "elastic": "auto (FP64, one CTA per QP)",
+                 "uneven": "auto (FP64; per size bin: one warp per QP for n <= 32, one CTA per QP above)"}[spec.kind]
     line = {
-        "metric": METRIC, "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_for(spec), "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": main_r["total_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "global_batch": B * world, "n": N, "m": M, "p": P,
-                   "precision": "auto (FP64; one warp per QP for n <= 32)", "parallelism": f"batch split x{world}",
-                   "l2": "flushed between steps (256 MB write), outside the per-step events"},
-        "roofline": roof, "gpu_launches": 2 * args.steps,
+        "config": config_for(spec, world, extra={
+            "precision": prec_desc, "parallelism": f"batch split x{world}",
+            "l2": "flushed between steps (256 MB write), outside the per-step events"}),
+        "roofline": roof, "gpu_launches": arm_main.launches * args.steps,
         "iterations": {"forward_mean": float(main_r["iters"].mean()), "relax_mean": float(main_r["riters"].mean()),
                        "converged": float(main_r["conv"].mean())},
         "clocks": main_r["clocks"],
         "forward_ms": main_r["fwd_ms"], "backward_ms": main_r["bwd_ms"],
     }
-    if "fp64_cta" in results and "mixed" in results:
+    if len(results) > 1:
         v = {k: world * B * args.steps / (r["total_ms"] * 1e-3) for k, r in results.items()}
-        line["variants"] = {
-            "fp64_one_cta_per_qp": {"value": v["fp64_cta"], "unit": "QPs/s",
-                                    "ms_per_step": results["fp64_cta"]["total_ms"] / args.steps},
-            "mixed_fp32_factor_fp64_refinement": {"value": v["mixed"], "unit": "QPs/s",
-                                                  "ms_per_step": results["mixed"]["total_ms"] / args.steps},
-        }
-        line["mixed_over_plain_fp64"] = v["mixed"] / v["fp64_cta"]
-        line["default_over_plain_fp64"] = v["auto"] / v["fp64_cta"]
+        names = {"fp64_cta": "fp64_one_cta_per_qp", "mixed": "mixed_fp32_factor_fp64_refinement"}
+        line["variants"] = {names[k]: {"value": v[k], "unit": "QPs/s", "ms_per_step": results[k]["total_ms"] /
+                                       args.steps} for k in results if k != "auto"}
+        plain = "fp64_cta" if "fp64_cta" in v else "auto"
+        if "mixed" in v:
+            line["mixed_over_plain_fp64"] = v["mixed"] / v[plain]
+        line["default_over_plain_fp64"] = v["auto"] / v[plain]
         line["converged_flags_identical"] = bool(all((r["conv"] == main_r["conv"]).all() for r in results.values()))
         line["iteration_counts_identical"] = bool(all((r["iters"] == main_r["iters"]).all()
                                                       for r in results.values()))
     if rank == 0 and not args.no_e2e:
-        line["e2e"] = run_e2e(args, data, dev)
+        line["e2e"] = run_e2e(args, spec, data, dev, arm_main)
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline_sample(data)
+        line["cpu_baseline"] = cpu_baseline(spec, data)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -376,8 +588,6 @@ def simt_peaks():
     fn = getattr(lib, "qpb_bench_fma_peak", None)
     if fn is None:
         return {"fp32_tflops": 75.0, "fp64_tflops": 37.0, "how": "nominal (no microbenchmark in the library)"}
-    import ctypes
-
     fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     fn.restype = ctypes.c_double
     out = {}
@@ -393,24 +603,63 @@ def simt_peaks():
     return out
 
 
-def run_e2e(args, data, dev):
+def run_e2e(args, spec: Spec, data, dev, arm):
     """Same metric through the public API from pinned host buffers: H2D of the
-    inputs and the incoming gradient, forward + backward, D2H of x and the six
+    inputs and the incoming gradient, forward + backward, D2H of x and the
     gradients, all inside the timed region."""
     import torch
 
     import qpax_b200 as qb
 
-    host = [torch.tensor(a).pin_memory() for a in data]
-    g_host = torch.full((B, N), 0.1, dtype=torch.float64).pin_memory()
-    outs_host = [torch.empty((B,) + s, dtype=torch.float64).pin_memory()
-                 for s in [(N,), (N, N), (N,), (M, N), (M,), (P, N), (P,)]]
-    h2d = sum(t.numel() * 8 for t in host) + g_host.numel() * 8
-    d2h = sum(t.numel() * 8 for t in outs_host)
+    B = spec.batch
+    if spec.kind == "uniform":
+        N, M, P = spec.n, spec.m, spec.p
+        host = [torch.tensor(a).pin_memory() for a in data]
+        g_host = torch.full((B, N), 0.1, dtype=torch.float64).pin_memory()
+        outs_host = [torch.empty((B,) + s, dtype=torch.float64).pin_memory()
+                     for s in [(N,), (N, N), (N,), (M, N), (M,), (P, N), (P,)]]
+        h2d = sum(t.numel() * 8 for t in host) + g_host.numel() * 8
+        d2h = sum(t.numel() * 8 for t in outs_host)
 
-    def step():
-        qb.solve_qp_primal_vjp_host(*host, g_host, TOL, KAPPA, out=outs_host, chunks=args.e2e_chunks)
+        def step():
+            qb.solve_qp_primal_vjp_host(*host, g_host, spec.tol, KAPPA, out=outs_host, chunks=args.e2e_chunks)
 
+        path = (f"qpax_b200.solve_qp_primal_vjp_host (C ABI): pinned host tensors, {args.e2e_chunks} chunks "
+                "pipelined over 3 streams (copy in / solve + backward / copy out overlap)")
+    elif spec.kind == "elastic":
+        host = [torch.tensor(a).pin_memory() for a in data] + [torch.full((B,), 1e3, dtype=torch.float64).pin_memory()]
+        g_host = torch.full((B, spec.n), 0.1, dtype=torch.float64).pin_memory()
+        shp = [(spec.n,), (spec.n, spec.n), (spec.n,), (spec.p, spec.n), (spec.p,)]
+        outs_host = [torch.empty((B,) + s, dtype=torch.float64).pin_memory() for s in shp]
+        h2d = sum(t.numel() * 8 for t in host) + g_host.numel() * 8
+        d2h = sum(t.numel() * 8 for t in outs_host)
+
+        def step():
+            d = [t.to(dev, non_blocking=True) for t in host + [g_host]]
+            x, grads = qb.solve_qp_elastic_primal_vjp(*d[:5], d[5], spec.tol, KAPPA)
+            for dst, src in zip(outs_host, (x,) + tuple(grads)):
+                dst.copy_(src, non_blocking=True)
+
+        path = "qpax_b200.solve_qp_elastic_primal_vjp (C ABI): pinned host tensors copied in and out on one stream"
+    else:
+        from qpax_b200.packed import pack
+
+        plan = arm.plan
+        host = [pack(v, torch.device("cpu")).pin_memory() for v in data]
+        g_host = torch.full((plan.totals[1],), 0.1, dtype=torch.float64).pin_memory()
+        outs_host = [torch.empty(plan.totals[1], dtype=torch.float64).pin_memory()] + \
+                    [torch.empty(plan.totals[k], dtype=torch.float64).pin_memory() for k in range(6)]
+        h2d = sum(t.numel() * 8 for t in host) + g_host.numel() * 8
+        d2h = sum(t.numel() * 8 for t in outs_host)
+
+        def step():
+            d = [t.to(dev, non_blocking=True) for t in host + [g_host]]
+            out = plan.solve(*d[:6], spec.tol)
+            grads = plan.primal_bwd(*d[:6], *out[:4], d[6], spec.tol, KAPPA)
+            for dst, src in zip(outs_host, (out[0],) + tuple(grads)):
+                dst.copy_(src, non_blocking=True)
+
+        path = "qpax_b200.PackedPlan (C ABI plan): packed pinned host tensors copied in and out on one stream"
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -422,9 +671,7 @@ def run_e2e(args, data, dev):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     return {"value": B * args.steps / (ms * 1e-3), "unit": "QPs/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps,
-            "path": f"qpax_b200.solve_qp_primal_vjp_host (C ABI): pinned host tensors, {args.e2e_chunks} chunks "
-                    "pipelined over 3 streams (copy in / solve + backward / copy out overlap)"}
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps, "path": path}
 
 
 def main():
@@ -433,19 +680,21 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dense")
     ap.add_argument("--only-default", action="store_true", help="time only the default (auto) path")
     ap.add_argument("--e2e-chunks", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    spec = WORKLOADS[args.workload]
     if args.impl == "reference":
         # host-only: rank 0 times the CPU implementation, other ranks exit
         world = int(os.environ.get("WORLD_SIZE", "1"))
-        run_reference(args, world, int(os.environ.get("RANK", "0")))
+        run_reference(args, spec, world, int(os.environ.get("RANK", "0")))
         return
     world, rank, local = dist_setup(args.gpus)
     try:
-        run_ours(args, world, rank, local)
+        run_ours(args, spec, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -189,13 +189,15 @@ int qpb_solve_qp_packed(const qpb_plan* plan, const double* Q, const double* q, 
                         qpb_stream_t stream);
 
 /* qpax/diff_qp.py:74-79 backward of solve_qp_primal over a packed batch
- * (gradients packed like Q, q, A, b, G, h). */
+ * (gradients packed like Q, q, A, b, G, h).  converged / iters (batch int32
+ * each, may be NULL) receive the relaxation's outcome per instance
+ * (qpax/pdip_relaxed.py:70-103). */
 int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const double* q, const double* A,
                                    const double* b, const double* G, const double* h, const double* x,
                                    const double* s, const double* z, const double* y, const double* dl_dx,
                                    double solver_tol, double target_kappa, double* dQ, double* dq, double* dA,
-                                   double* db, double* dG, double* dh, void* workspace, size_t workspace_bytes,
-                                   qpb_stream_t stream);
+                                   double* db, double* dG, double* dh, int32_t* converged, int32_t* iters,
+                                   void* workspace, size_t workspace_bytes, qpb_stream_t stream);
 
 /* qpb_solve_qp for callers that cannot allocate device memory.  No
  * counterpart in qpax: it exists for hosts where a solve must not call

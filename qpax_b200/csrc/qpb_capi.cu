@@ -155,6 +155,10 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   if (NT == 256 && KC < 4) NT = 128;
   KernelFn fn = pick_kernel(elastic, mixed, NT, KC);
   if (!fn) return QPB_ERR_UNSUPPORTED;
+  // dynamic shared memory left beside the kernel's static staging
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, (const void*)fn) != cudaSuccess) return QPB_ERR_CUDA;
+  const size_t team_budget = smem_budget > fa.sharedSizeBytes ? smem_budget - fa.sharedSizeBytes : 0;
   size_t arena = elastic ? ElasticArena::bytes(d.n, d.p, mixed) : StdArena::bytes(d.n, d.m, d.p, mixed);
   arena = (arena + 255) & ~size_t(255);
   pl->fn = (const void*)fn;
@@ -163,10 +167,10 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   int teams = 1;
   if (NT == 32) {
     // several warp teams per CTA, as many as fit (up to 8)
-    teams = (int)(smem_budget / arena);
+    teams = (int)(team_budget / arena);
     teams = teams > 8 ? 8 : teams;
   }
-  if (teams >= 1 && arena * teams <= smem_budget) {
+  if (teams >= 1 && arena * teams <= team_budget) {
     pl->in_smem = 1;
     pl->teams = teams;
     pl->smem_bytes = arena * teams;

@@ -53,13 +53,46 @@ struct Core {
   int max_sweeps;
   int use64;
   int st_f32, st_f64, st_sweeps, st_flags;
+  BlockedStage* st;  // shared staging of the blocked FP64 path (teams of >= 2 warps)
+
+  // FP64 factors: teams of one warp keep the split layout (L, Y, F) and
+  // per-column elimination; larger teams factor the whole KKT matrix blocked
+  // on the FP64 tensor cores (qpb_blocked.cuh).
+  static constexpr bool kBlocked = NT > 32;
 
   QPB_DEV void reset_stats() { st_f32 = st_f64 = st_sweeps = st_flags = 0; use64 = 0; }
 
   QPB_NOINLINE void factor64() {
-    const double r = factor_kkt<NT, KC, double>(t, n, m, p, c.Q, c.G, c.A, ld, c.w, nullptr, c.fr.view<double>());
+    double r;
+    if constexpr (kBlocked) {
+      const KKTView f = KKTRegion::view(c.fr.base, n, m);
+      form_kkt<NT>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w);
+      t.sync();
+      r = kkt_factor<NT>(t, f, st);
+    } else {
+      r = factor_kkt<NT, KC, double>(t, n, m, p, c.Q, c.G, c.A, ld, c.w, nullptr, c.fr.view<double>());
+    }
     st_f64++;
     if (!(r < INFINITY)) st_flags |= kFlagBreakdown64;
+  }
+
+  // [H A'; A 0][dx; dy] = [rhs; v4] with the blocked FP64 factor.
+  QPB_NOINLINE void reduced_blocked(const double* rhs, const double* v4, double* dx, double* dy) {
+    const KKTView f = KKTRegion::view(c.fr.base, n, m);
+    double* v = st->v;
+    for (int i = t.r; i < f.N; i += NT) {
+      double x = 0.0;
+      if (i < n)
+        x = rhs[i];
+      else if (i >= f.n8 && i - f.n8 < m)
+        x = v4[i - f.n8];
+      v[i] = x;
+    }
+    t.sync();
+    kkt_solve<NT>(t, f, v, st);
+    for (int i = t.r; i < n; i += NT) dx[i] = v[i];
+    for (int i = t.r; i < m; i += NT) dy[i] = v[f.n8 + i];
+    t.sync();
   }
 
   // Factor for the weights currently in c.w.
@@ -145,8 +178,12 @@ struct Core {
         factor64();
       }
     }
-    if (t.warp() == 0) reduced_solve_warp<KC, double>(c.fr.view<double>(), n, m, rhs, v4, dx, dy, t.lane());
-    t.sync();
+    if constexpr (kBlocked) {
+      reduced_blocked(rhs, v4, dx, dy);
+    } else {
+      if (t.warp() == 0) reduced_solve_warp<KC, double>(c.fr.view<double>(), n, m, rhs, v4, dx, dy, t.lane());
+      t.sync();
+    }
   }
 
   // min over the team's entries of -v/d for d < 0 (qpax/pdip.py:66-73 before the cap at 1).

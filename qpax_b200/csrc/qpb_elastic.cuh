@@ -57,7 +57,7 @@ struct ElasticQP {
 
   QPB_DEV const Team<NT>& T() const { return k.t; }
 
-  QPB_DEV void setup(const Params& prm, unsigned char* arena, int rank) {
+  QPB_DEV void setup(const Params& prm, unsigned char* arena, int rank, BlockedStage* stage) {
     P = &prm;
     n = prm.n; p = prm.p;
     a.carve(reinterpret_cast<uintptr_t>(arena), n, p, kMixed);
@@ -66,6 +66,7 @@ struct ElasticQP {
     k.c = a;
     k.t.r = rank;
     k.t.red = a.red;
+    k.st = stage;
     k.pivot_max = prm.pivot_max;
     k.max_sweeps = prm.max_sweeps;
   }

@@ -9,7 +9,7 @@ namespace qpb {
 // Persistent: each team pulls instance indices from P.counter until the
 // batch is exhausted (a bounded loop: at most `batch` fetches in total).
 template <class Solver, int NT>
-__global__ void __launch_bounds__(256) ipm_kernel(const __grid_constant__ Params P) {
+__global__ void __launch_bounds__(256, 1) ipm_kernel(const __grid_constant__ Params P) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int next_inst;
   const int teams = blockDim.x / NT;
@@ -18,8 +18,13 @@ __global__ void __launch_bounds__(256) ipm_kernel(const __grid_constant__ Params
   unsigned char* arena = P.arena_in_smem
                              ? smem + (size_t)team * P.arena_bytes
                              : P.arena + ((size_t)blockIdx.x * teams + team) * P.arena_bytes;
+  BlockedStage* stage = nullptr;
+  if constexpr (NT > 32) {  // one team per CTA: the blocked FP64 path's staging
+    __shared__ BlockedStage blocked_stage;
+    stage = &blocked_stage;
+  }
   Solver S;
-  S.setup(P, arena, rank);
+  S.setup(P, arena, rank, stage);
   for (;;) {
     int inst;
     if constexpr (NT == 32) {

@@ -2,6 +2,7 @@
 // H = Q + G^T diag(w) G, its LDL^T factor, the Schur complement on A, and
 // the reduced solve used by every Newton / predictor-corrector step.
 #pragma once
+#include "qpb_blocked.cuh"
 #include "qpb_team.cuh"
 
 namespace qpb {
@@ -33,7 +34,8 @@ struct Factor {
   int ldl, ldy, ldf;
 };
 
-// A factor region sized for doubles; a float view reuses the same bytes.
+// A factor region sized for doubles; a float view reuses the same bytes, and
+// so does the blocked FP64 view of the whole KKT matrix (KKTRegion).
 struct FactorRegion {
   unsigned char* base;
   int n, m;
@@ -44,7 +46,8 @@ struct FactorRegion {
     c.take<double>((size_t)m * pad4(n));
     c.take<double>((size_t)m * odd_ld(m));
     c.take<double>(m);
-    return c.cur + 16;
+    const size_t split = c.cur + 16, whole = KKTRegion::bytes(n, m);
+    return split > whole ? split : whole;
   }
   template <class R>
   __device__ Factor<R> view() const {

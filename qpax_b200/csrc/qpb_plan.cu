@@ -277,8 +277,8 @@ int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const 
                                    const double* b, const double* G, const double* h, const double* x,
                                    const double* s, const double* z, const double* y, const double* dl_dx,
                                    double solver_tol, double target_kappa, double* dQ, double* dq, double* dA,
-                                   double* db, double* dG, double* dh, void* workspace, size_t workspace_bytes,
-                                   qpb_stream_t stream) {
+                                   double* db, double* dG, double* dh, int32_t* converged, int32_t* iters,
+                                   void* workspace, size_t workspace_bytes, qpb_stream_t stream) {
   if (!plan) return QPB_ERR_INVALID_ARGUMENT;
   const int64_t* t = plan->totals;
   if (!ok_ptr(Q, t[0]) || !ok_ptr(q, t[1]) || !ok_ptr(A, t[2]) || !ok_ptr(b, t[3]) || !ok_ptr(G, t[4]) ||
@@ -294,6 +294,8 @@ int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const 
   P.in[0] = x; P.in[1] = s; P.in[2] = z; P.in[3] = y;
   P.gx = dl_dx;
   P.dQ = dQ; P.dq = dq; P.dA = dA; P.db = db; P.dG = dG; P.dh = dh;
+  P.conv = converged;
+  P.iters = iters;
   return launch_packed(plan, P, workspace, workspace_bytes, stream);
 }
 

@@ -54,7 +54,7 @@ struct StdQP {
 
   QPB_DEV const Team<NT>& t() const { return k.t; }
 
-  QPB_DEV void setup(const Params& prm, unsigned char* arena, int rank) {
+  QPB_DEV void setup(const Params& prm, unsigned char* arena, int rank, BlockedStage* stage) {
     P = &prm;
     arena_base = arena;
     n = prm.n; m = prm.m; p = prm.p;
@@ -64,6 +64,7 @@ struct StdQP {
     k.c = a;  // slices CoreArena
     k.t.r = rank;
     k.t.red = a.red;
+    k.st = stage;
     k.pivot_max = prm.pivot_max;
     k.max_sweeps = prm.max_sweeps;
   }

@@ -32,7 +32,7 @@ _SIGS = {
     "qpb_solve_qp_packed": ([ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_double] + [ctypes.c_void_p] * 6 +
                             [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p], ctypes.c_int),
     "qpb_solve_qp_primal_bwd_packed": ([ctypes.c_void_p] + [ctypes.c_void_p] * 11 + [ctypes.c_double] * 2 +
-                                       [ctypes.c_void_p] * 6 + [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+                                       [ctypes.c_void_p] * 8 + [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
                                        ctypes.c_int),
 }
 
@@ -116,13 +116,18 @@ class PackedPlan:
         return x, s, z, y, conv, iters
 
     def primal_bwd(self, Q, q, A, b, G, h, x, s, z, y, dl_dx, solver_tol: float = 1e-5,
-                   target_kappa: float = 1e-3):
-        """qpb_solve_qp_primal_bwd_packed -> packed (dQ, dq, dA, db, dG, dh)."""
+                   target_kappa: float = 1e-3, relax_out=None):
+        """qpb_solve_qp_primal_bwd_packed -> packed (dQ, dq, dA, db, dG, dh).
+
+        relax_out: optional (converged, iters) int32 device tensors of length
+        batch that receive the relaxation's per-instance outcome."""
         grads = [self.new(k) for k in range(6)]
+        rc, ri = relax_out if relax_out is not None else (None, None)
         wp, wb = self._ws()
         _lib.call("qpb_solve_qp_primal_bwd_packed", self.handle,
                   *[_lib.ptr(t) for t in (Q, q, A, b, G, h, x, s, z, y, dl_dx)], ctypes.c_double(solver_tol),
-                  ctypes.c_double(target_kappa), *[_lib.ptr(t) for t in grads], wp, wb, _lib.stream_handle())
+                  ctypes.c_double(target_kappa), *[_lib.ptr(t) for t in grads], _lib.ptr(rc), _lib.ptr(ri),
+                  wp, wb, _lib.stream_handle())
         return tuple(grads)
 
 
