@@ -275,7 +275,7 @@ def run_reference(args, spec: Spec, world, rank):
     B = spec.batch
     # each step is a bounded sample of the workload: the whole batch when it
     # is cheap on the host, else a fixed in-order slice of it
-    per_step = {"uneven": 512, "elastic": 1024}.get(spec.kind, B)
+    per_step = {"uneven": 128, "elastic": 256}.get(spec.kind, B)
     per_step = min(per_step, B)
     step = lambda: _oracle_chunk(spec, data, 0, per_step, 0)
     for _ in range(args.warmup):

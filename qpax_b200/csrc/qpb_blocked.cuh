@@ -29,6 +29,7 @@ namespace qpb {
 constexpr int kPanel = 32;
 constexpr int kMaxDim = 256;  // n <= 256, m <= 256
 constexpr int kLdStride = kPanel + 2;
+constexpr int kPanelLd = kPanel + 4;  // row stride of a staged panel: 4 (mod 16)
 
 __host__ __device__ inline int pad8(int n) { return (n + 7) & ~7; }
 // Row stride of K: 4 (mod 16) doubles, so that the 8 x 4 fragment loads of a
@@ -87,62 +88,152 @@ QPB_DEV void tri_pair(int tau, int& bi, int& bj) {
   bj = tau - r * (r + 1) / 2;
 }
 
+// Row stride (doubles) of a chunk of G staged in shared memory: 4 (mod 16),
+// so the 8 x 4 fragment reads of a warp are free of bank conflicts.
+__host__ __device__ inline int gstage_ld(int ldg) { return ((ldg + 15) & ~15) + 4; }
+// Bytes of the two chunk buffers (rows x gstage_ld doubles of G, then rows
+// weights, each).
+__host__ __device__ inline size_t gstage_bytes(int ldg, int rows) {
+  return 2 * (size_t)rows * (gstage_ld(ldg) + 1) * sizeof(double) + 64;
+}
+
+QPB_DEV void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+QPB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int kPending>
+QPB_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory"); }
+
+// Lower entries of one 32 x 32 block (bi, bj) of H = sym(Q) + G' diag(w) G
+// from the accumulated G' diag(w) G tiles; entries beyond n are identity.
+QPB_DEV void store_h_block(const KKTView& f, const double* Q, int ldq, int bi, int bj, int nti, int ntj,
+                           const double (&acc)[4][4][2], int g, int tg) {
+  const int n = f.n;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      if (!(a < nti && b < ntj)) continue;
+      const int i = 32 * bi + 8 * a + g;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int j = 32 * bj + 8 * b + 2 * tg + e;
+        if (j > i) continue;
+        double v;
+        if (i < n && j < n)
+          v = 0.5 * (Q[(size_t)i * ldq + j] + Q[(size_t)j * ldq + i]) + acc[a][b][e];
+        else
+          v = (i == j) ? 1.0 : 0.0;
+        f.K[(size_t)i * f.ld + j] = v;
+      }
+    }
+}
+
+// The (up to) 16 tensor-core tiles of one k-step of a block: A rows from
+// w_k G[k, i-cols], B columns from G[k, j-cols]; `row` points at G[k, 0].
+QPB_DEV void h_block_kstep(double (&acc)[4][4][2], const double* row, double wk, bool in, int n, int i0, int j0,
+                           int nti, int ntj, bool diag, int g) {
+  double av[4], bv[4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int ci = i0 + 8 * a + g, cj = j0 + 8 * a + g;
+    av[a] = (in && a < nti && ci < n) ? wk * row[ci] : 0.0;
+    bv[a] = (in && a < ntj && cj < n) ? row[cj] : 0.0;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      if (a < nti && b < ntj && (!diag || b <= a)) mma884(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+}
+
 // K <- [sym(Q) + G' diag(w) G, A'; A, 0] (lower triangle, padded).  G, A, Q
-// are row-major with leading dimensions ldg, lda, ldq; rows of G beyond p
-// and columns beyond n read as zero.
+// are row-major with leading dimensions ldg, lda, ldq (ldg a multiple of 4);
+// rows of G beyond p and columns beyond n read as zero.  H is computed in
+// 32 x 32 blocks, one per warp.  With `gbuf` (shared memory of
+// gstage_bytes(ldg, KR)), the warps take their blocks in rounds and stream G
+// through two chunk buffers of KR rows (cp.async double buffering), so each
+// row of G crosses from L2 once per round instead of once per block;
+// without it, fragments are read from G in place (G in shared memory).
 template <int NT>
 QPB_NOINLINE void form_kkt(const Team<NT>& t, const KKTView& f, int p, const double* Q, int ldq, const double* G,
-                           int ldg, const double* A, int lda, const double* wv) {
+                           int ldg, const double* A, int lda, const double* wv, double* gbuf, int KR) {
+  constexpr int kWarps = NT / 32;
   const int n = f.n, n8 = f.n8, ld = f.ld;
   const int lane = t.lane(), g = lane >> 2, tg = lane & 3;
   const int nb = (n8 + 31) >> 5;
   const int npairs = nb * (nb + 1) / 2;
-  for (int tau = t.warp(); tau < npairs; tau += NT / 32) {
-    int bi, bj;
-    tri_pair(tau, bi, bj);
-    const int i0 = 32 * bi, j0 = 32 * bj;
-    const int nti = min(4, (n8 - i0) >> 3), ntj = min(4, (n8 - j0) >> 3);
-    double acc[4][4][2];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-    for (int k0 = 0; k0 < p; k0 += 4) {
-      const int k = k0 + tg;
-      const bool in = k < p;
-      const double* row = G + (size_t)(in ? k : 0) * ldg;
-      const double wk = in ? wv[k] : 0.0;
-      double av[4], bv[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int ci = i0 + 8 * a + g, cj = j0 + 8 * a + g;
-        av[a] = (a < nti && ci < n) ? wk * row[ci] : 0.0;
-        bv[a] = (a < ntj && cj < n && in) ? row[cj] : 0.0;
+  if (gbuf == nullptr) {
+    for (int tau = t.warp(); tau < npairs; tau += kWarps) {
+      int bi, bj;
+      tri_pair(tau, bi, bj);
+      const int nti = min(4, (n8 - 32 * bi) >> 3), ntj = min(4, (n8 - 32 * bj) >> 3);
+      double acc[4][4][2] = {};
+      for (int k0 = 0; k0 < p; k0 += 4) {
+        const int k = k0 + tg;
+        const bool in = k < p;
+        h_block_kstep(acc, G + (size_t)(in ? k : 0) * ldg, in ? wv[k] : 0.0, in, n, 32 * bi, 32 * bj, nti, ntj,
+                      bi == bj, g);
       }
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (a < nti && b < ntj && (bi != bj || b <= a)) mma884(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+      store_h_block(f, Q, ldq, bi, bj, nti, ntj, acc, g, tg);
     }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        if (!(a < nti && b < ntj)) continue;
-        const int i = i0 + 8 * a + g;
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int j = j0 + 8 * b + 2 * tg + e;
-          if (j > i) continue;
-          double v;
-          if (i < n && j < n)
-            v = 0.5 * (Q[(size_t)i * ldq + j] + Q[(size_t)j * ldq + i]) + acc[a][b][e];
-          else
-            v = (i == j) ? 1.0 : 0.0;
-          f.K[(size_t)i * ld + j] = v;
-        }
+  } else {
+    const int lds = gstage_ld(ldg);
+    const int units = ldg >> 1;  // 16-byte pieces per row
+    const int nch = (p + KR - 1) / KR;
+    double* wbuf = gbuf + (size_t)2 * KR * lds;  // weights of the two chunks
+    auto issue = [&](int ch) {
+      double* dst = gbuf + (size_t)(ch & 1) * KR * lds;
+      const int k0 = ch * KR, rows = min(KR, p - k0);
+      for (int e = t.r; e < rows * units; e += NT) {
+        const int r = e / units, u = e - r * units;
+        cp_async16(dst + (size_t)r * lds + 2 * u, G + (size_t)(k0 + r) * ldg + 2 * u);
       }
+      // weights in whole 16-byte pieces (k0 is even): with an odd count the
+      // last piece also copies the double after w[p - 1] -- the next array
+      // of the arena -- which is never read
+      double* wd = wbuf + (ch & 1) * KR;
+      for (int e = t.r; 2 * e < rows; e += NT) cp_async16(wd + 2 * e, wv + k0 + 2 * e);
+    };
+    for (int base = 0; base < npairs; base += kWarps) {
+      const int tau = base + t.warp();
+      const bool active = tau < npairs;
+      int bi = 0, bj = 0;
+      if (active) tri_pair(tau, bi, bj);
+      const int nti = active ? min(4, (n8 - 32 * bi) >> 3) : 0;
+      const int ntj = active ? min(4, (n8 - 32 * bj) >> 3) : 0;
+      double acc[4][4][2] = {};
+      if (nch > 0) issue(0);
+      cp_async_commit();
+      for (int ch = 0; ch < nch; ++ch) {
+        if (ch + 1 < nch) issue(ch + 1);
+        cp_async_commit();
+        cp_async_wait<1>();  // this thread's copies of chunk ch have landed
+        t.sync();            // and everyone else's
+        if (active) {
+          const double* buf = gbuf + (size_t)(ch & 1) * KR * lds;
+          const double* wb = wbuf + (ch & 1) * KR;
+          const int rows = min(KR, p - ch * KR);
+          if (rows == KR) {
+#pragma unroll 4
+            for (int kk = 0; kk < KR; kk += 4) {
+              const int r = kk + tg;
+              h_block_kstep(acc, buf + (size_t)r * lds, wb[r], true, n, 32 * bi, 32 * bj, nti, ntj, bi == bj, g);
+            }
+          } else {
+            for (int kk = 0; kk < rows; kk += 4) {
+              const int r = kk + tg;
+              const bool in = r < rows;
+              h_block_kstep(acc, buf + (size_t)(in ? r : 0) * lds, in ? wb[r] : 0.0, in, n, 32 * bi, 32 * bj,
+                            nti, ntj, bi == bj, g);
+            }
+          }
+        }
+        t.sync();  // chunk ch is read before chunk ch + 2 overwrites its buffer
+      }
+      if (active) store_h_block(f, Q, ldq, bi, bj, nti, ntj, acc, g, tg);
+    }
   }
   // A rows (and the zero (2,2) block)
   const int m = f.m, m8 = f.m8;
@@ -223,7 +314,7 @@ QPB_DEV void diag_factor(const KKTView& f, int J0, int w, int real_end, int sign
 // are updated too).  sign = -1 stores dinv = -1/d (the (2,2) block of K_K).
 template <int NT>
 QPB_DEV void ldlt_phase(const Team<NT>& t, const KKTView& f, int J0s, int J0e, int real_end, int sign,
-                        BlockedStage* st, double& dmin, double& dmax, int& bad) {
+                        BlockedStage* st, double* pbuf, size_t pcap, double& dmin, double& dmax, int& bad) {
   double* K = f.K;
   const int ld = f.ld, N = f.N;
   const int lane = t.lane(), g = lane >> 2, tg = lane & 3;
@@ -232,6 +323,11 @@ QPB_DEV void ldlt_phase(const Team<NT>& t, const KKTView& f, int J0s, int J0e, i
     if (t.warp() == 0) diag_factor(f, J0, w, real_end, sign, st, lane, dmin, dmax, bad);
     t.sync();
     const int T0 = J0 + w;
+    // With a shared-memory panel buffer large enough, the panel's L rows are
+    // also written there and the trailing update reads its fragments from it.
+    const bool use_p = pbuf != nullptr && (size_t)(N - T0) * kPanelLd <= pcap;
+    const double* Ls = use_p ? pbuf : K + (size_t)T0 * ld + J0;  // L[T0 + r][J0 + c] at Ls[r * lls + c]
+    const int lls = use_p ? kPanelLd : ld;
     // panel rows below: L[i][J] = (H[i][J] L_JJ^-T) D_J^-1, one row per thread
     for (int i = T0 + t.r; i < N; i += NT) {
       double* Ki = K + (size_t)i * ld + J0;
@@ -253,9 +349,15 @@ QPB_DEV void ldlt_phase(const Team<NT>& t, const KKTView& f, int J0s, int J0e, i
           u[c] = s0 + s1;
         }
       }
+      double* Pi = use_p ? pbuf + (size_t)(i - T0) * kPanelLd : nullptr;
 #pragma unroll
-      for (int c = 0; c < kPanel; ++c)
-        if (c < w) Ki[c] = u[c] * st->Di[c];
+      for (int c = 0; c < kPanel; ++c) {
+        if (c < w) {
+          const double l = u[c] * st->Di[c];
+          Ki[c] = l;
+          if (use_p) Pi[c] = l;
+        }
+      }
     }
     t.sync();
     // trailing update of the lower triangle K[T0:N, T0:N] -= L_J D_J L_J'
@@ -281,13 +383,13 @@ QPB_DEV void ldlt_phase(const Team<NT>& t, const KKTView& f, int J0s, int J0e, i
             }
           }
         for (int kk = 0; kk < w; kk += 4) {
-          const int k = J0 + kk + tg;
-          const double dk = st->Dd[kk + tg];
+          const int k = kk + tg;
+          const double dk = st->Dd[k];
           double av[4], bv[4];
 #pragma unroll
           for (int a = 0; a < 4; ++a) {
-            av[a] = (a < nti) ? -K[(size_t)(i0 + 8 * a + g) * ld + k] * dk : 0.0;
-            bv[a] = (a < ntj) ? K[(size_t)(j0 + 8 * a + g) * ld + k] : 0.0;
+            av[a] = (a < nti) ? -Ls[(size_t)(i0 - T0 + 8 * a + g) * lls + k] * dk : 0.0;
+            bv[a] = (a < ntj) ? Ls[(size_t)(j0 - T0 + 8 * a + g) * lls + k] : 0.0;
           }
 #pragma unroll
           for (int a = 0; a < 4; ++a)
@@ -315,10 +417,10 @@ QPB_DEV void ldlt_phase(const Team<NT>& t, const KKTView& f, int J0s, int J0e, i
 // Factor K (already formed).  Returns the pivot ratio max(D)/min(D) of H, or
 // +inf when a pivot of H or of F is not strictly positive and finite.
 template <int NT>
-QPB_NOINLINE double kkt_factor(const Team<NT>& t, const KKTView& f, BlockedStage* st) {
+QPB_NOINLINE double kkt_factor(const Team<NT>& t, const KKTView& f, BlockedStage* st, double* pbuf, size_t pcap) {
   double dmin = INFINITY, dmax = 0.0;
   int bad = 0;
-  ldlt_phase<NT>(t, f, 0, f.n8, f.n, 1, st, dmin, dmax, bad);
+  ldlt_phase<NT>(t, f, 0, f.n8, f.n, 1, st, pbuf, pcap, dmin, dmax, bad);
   double fmin = INFINITY, fmax = 0.0;
   int fbad = 0;
   if (f.m8 > 0) {
@@ -331,7 +433,7 @@ QPB_NOINLINE double kkt_factor(const Team<NT>& t, const KKTView& f, BlockedStage
       *x = (r >= f.m && r == c) ? 1.0 : -*x;
     }
     t.sync();
-    ldlt_phase<NT>(t, f, n8, f.N, n8 + f.m, -1, st, fmin, fmax, fbad);
+    ldlt_phase<NT>(t, f, n8, f.N, n8 + f.m, -1, st, pbuf, pcap, fmin, fmax, fbad);
   }
   bad = t.any(bad | fbad);
   dmin = t.min(dmin);

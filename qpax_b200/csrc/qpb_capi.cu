@@ -79,7 +79,9 @@ static int occupancy(const void* fn, int threads, size_t smem, int* per_sm) {
       *per_sm = vals[i];
       return QPB_OK;
     }
-  if (smem > 48 * 1024) {
+  // the default dynamic limit is 48 KB minus the kernel's static shared
+  // memory, so raise it for any request
+  if (smem > 0) {
     int li = -1;
     for (int i = 0; i < nlimits; ++i)
       if (limits[i].dev == dev && limits[i].fn == fn) li = i;
@@ -118,6 +120,7 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   const bool mixed = cfg.precision == QPB_PRECISION_MIXED;
   const DevInfo di = dev_info();
   if (!di.ok) return QPB_ERR_CUDA;
+  pl->gstage_rows = 0;
   const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
   const int np = warp_np(d);
   if (!elastic && !mixed && np && (cfg.team_threads == 0 || cfg.team_threads == 32)) {
@@ -178,6 +181,18 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     pl->in_smem = 0;
     pl->teams = NT == 32 ? 4 : 1;
     pl->smem_bytes = 0;
+    if (NT > 32 && d.p > 0 && !mixed) {
+      // stream G through shared memory in chunks of up to 32 rows
+      const int ldg = (d.n + 3) & ~3;
+      for (int rows = 32; rows >= 8; rows >>= 1) {
+        const size_t b = gstage_bytes(ldg, rows);
+        if (b <= team_budget) {
+          pl->gstage_rows = rows;
+          pl->smem_bytes = b;
+          break;
+        }
+      }
+    }
   }
   pl->threads = NT * pl->teams;
   int per_sm = 0;
@@ -249,6 +264,7 @@ static int launch(Params P, const qpb_dims* d, const qpb_config* cfg, void* ws, 
   P.arena = reinterpret_cast<unsigned char*>(ws) + kCounterBytes;
   P.arena_bytes = pl.arena_bytes;
   P.arena_in_smem = pl.in_smem;
+  P.gstage_rows = pl.gstage_rows;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(ws, 0, sizeof(int), s) != cudaSuccess) return QPB_ERR_CUDA;
   void* args[] = {&P};

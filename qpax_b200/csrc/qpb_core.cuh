@@ -54,6 +54,8 @@ struct Core {
   int use64;
   int st_f32, st_f64, st_sweeps, st_flags;
   BlockedStage* st;  // shared staging of the blocked FP64 path (teams of >= 2 warps)
+  double* gbuf = nullptr;  // G chunk buffers in shared memory (arena in global memory), or none
+  int gstage_rows = 0;
 
   // FP64 factors: teams of one warp keep the split layout (L, Y, F) and
   // per-column elimination; larger teams factor the whole KKT matrix blocked
@@ -66,9 +68,11 @@ struct Core {
     double r;
     if constexpr (kBlocked) {
       const KKTView f = KKTRegion::view(c.fr.base, n, m);
-      form_kkt<NT>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w);
+      form_kkt<NT>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w, gbuf, gstage_rows);
       t.sync();
-      r = kkt_factor<NT>(t, f, st);
+      // the G chunk buffers are free again: they hold the factor's panels
+      const size_t pcap = gbuf ? (gstage_bytes(ld, gstage_rows) - 64) / sizeof(double) : 0;
+      r = kkt_factor<NT>(t, f, st, gbuf, pcap);
     } else {
       r = factor_kkt<NT, KC, double>(t, n, m, p, c.Q, c.G, c.A, ld, c.w, nullptr, c.fr.view<double>());
     }

@@ -17,6 +17,7 @@ struct Plan {
   int NT, threads, teams, grid;
   size_t arena_bytes, smem_bytes, ws_bytes;
   int in_smem;
+  int gstage_rows;  // rows of G per shared-memory chunk (arena in global memory), 0: none
 };
 
 int warp_np(const qpb_dims& d);

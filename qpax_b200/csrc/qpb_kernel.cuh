@@ -25,6 +25,13 @@ __global__ void __launch_bounds__(256, 1) ipm_kernel(const __grid_constant__ Par
   }
   Solver S;
   S.setup(P, arena, rank, stage);
+  if constexpr (NT > 32) {
+    // arena in global memory: dynamic shared memory holds the G chunk buffers
+    if (!P.arena_in_smem && P.gstage_rows > 0) {
+      S.k.gbuf = reinterpret_cast<double*>(smem);
+      S.k.gstage_rows = P.gstage_rows;
+    }
+  }
   for (;;) {
     int inst;
     if constexpr (NT == 32) {

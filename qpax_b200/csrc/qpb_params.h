@@ -45,6 +45,7 @@ struct Params {
   unsigned char *arena; // global arenas when they do not fit in shared memory
   size_t arena_bytes;   // bytes per team arena
   int arena_in_smem;
+  int gstage_rows;      // global arenas: rows of G per chunk staged in dynamic shared memory (0: none)
   int *counter;         // work counter (zeroed before launch)
   // Packed (uneven) batches: when `shapes` is set, instance i has its own
   // (n, m, p) = shapes[3i..3i+2] and element offsets offs[6i..6i+5] into the

@@ -230,6 +230,7 @@ static int launch_packed(const qpb_plan* pl, Params P, void* ws, size_t ws_bytes
     Q.arena = wsb + kCounterBytes;
     Q.arena_bytes = b.launch.arena_bytes;
     Q.arena_in_smem = b.launch.in_smem;
+    Q.gstage_rows = b.launch.gstage_rows;
     if (cudaMemsetAsync(wsb, 0, sizeof(int), s) != cudaSuccess) return QPB_ERR_CUDA;
     void* args[] = {&Q};
     if (cudaLaunchKernel(b.launch.fn, dim3(b.launch.grid), dim3(b.launch.threads), args, b.launch.smem_bytes, s) !=
