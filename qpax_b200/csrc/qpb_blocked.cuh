@@ -73,10 +73,12 @@ struct KKTRegion {
   }
 };
 
+// D += A B on the FP64 tensor cores (no side effects beyond d0, d1, so the
+// compiler may schedule fragment loads around it).
 QPB_DEV void mma884(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
 }
 
 // Block pair (bi >= bj) of the lower triangle of an nb x nb block grid.
@@ -105,8 +107,9 @@ QPB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memo
 template <int kPending>
 QPB_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory"); }
 
-// Lower entries of one 32 x 32 block (bi, bj) of H = sym(Q) + G' diag(w) G
-// from the accumulated G' diag(w) G tiles; entries beyond n are identity.
+// Lower entries of one 32 x 32 block (bi, bj) of H = Q + G' diag(w) G (Q
+// symmetric) from the accumulated G' diag(w) G tiles; entries beyond n are
+// identity.
 QPB_DEV void store_h_block(const KKTView& f, const double* Q, int ldq, int bi, int bj, int nti, int ntj,
                            const double (&acc)[4][4][2], int g, int tg) {
   const int n = f.n;
@@ -122,7 +125,7 @@ QPB_DEV void store_h_block(const KKTView& f, const double* Q, int ldq, int bi, i
         if (j > i) continue;
         double v;
         if (i < n && j < n)
-          v = 0.5 * (Q[(size_t)i * ldq + j] + Q[(size_t)j * ldq + i]) + acc[a][b][e];
+          v = Q[(size_t)i * ldq + j] + acc[a][b][e];  // Q was symmetrized when loaded
         else
           v = (i == j) ? 1.0 : 0.0;
         f.K[(size_t)i * f.ld + j] = v;
@@ -130,22 +133,32 @@ QPB_DEV void store_h_block(const KKTView& f, const double* Q, int ldq, int bi, i
     }
 }
 
-// The (up to) 16 tensor-core tiles of one k-step of a block: A rows from
-// w_k G[k, i-cols], B columns from G[k, j-cols]; `row` points at G[k, 0].
-QPB_DEV void h_block_kstep(double (&acc)[4][4][2], const double* row, double wk, bool in, int n, int i0, int j0,
-                           int nti, int ntj, bool diag, int g) {
-  double av[4], bv[4];
+// Fragments of one k-step of a block: A rows from w_k G[k, i-cols], B
+// columns from G[k, j-cols]; `row` points at G[k, 0].
+QPB_DEV void h_frags(double (&av)[4], double (&bv)[4], const double* row, double wk, bool in, int n, int i0, int j0,
+                     int nti, int ntj, int g) {
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const int ci = i0 + 8 * a + g, cj = j0 + 8 * a + g;
     av[a] = (in && a < nti && ci < n) ? wk * row[ci] : 0.0;
     bv[a] = (in && a < ntj && cj < n) ? row[cj] : 0.0;
   }
+}
+// The (up to) 16 tensor-core tiles of one k-step (lower ones only on a
+// diagonal block).
+QPB_DEV void h_mmas(double (&acc)[4][4][2], const double (&av)[4], const double (&bv)[4], int nti, int ntj,
+                    bool diag) {
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b)
       if (a < nti && b < ntj && (!diag || b <= a)) mma884(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+}
+QPB_DEV void h_block_kstep(double (&acc)[4][4][2], const double* row, double wk, bool in, int n, int i0, int j0,
+                           int nti, int ntj, bool diag, int g) {
+  double av[4], bv[4];
+  h_frags(av, bv, row, wk, in, n, i0, j0, nti, ntj, g);
+  h_mmas(acc, av, bv, nti, ntj, diag);
 }
 
 // K <- [sym(Q) + G' diag(w) G, A'; A, 0] (lower triangle, padded).  G, A, Q
@@ -215,11 +228,25 @@ QPB_NOINLINE void form_kkt(const Team<NT>& t, const KKTView& f, int p, const dou
           const double* buf = gbuf + (size_t)(ch & 1) * KR * lds;
           const double* wb = wbuf + (ch & 1) * KR;
           const int rows = min(KR, p - ch * KR);
-          if (rows == KR) {
-#pragma unroll 4
-            for (int kk = 0; kk < KR; kk += 4) {
-              const int r = kk + tg;
-              h_block_kstep(acc, buf + (size_t)r * lds, wb[r], true, n, 32 * bi, 32 * bj, nti, ntj, bi == bj, g);
+          if (rows == 32 && KR == 32) {
+            // full chunk: the next k-step's fragments load under this one's MMAs
+            double av[4], bv[4];
+            h_frags(av, bv, buf + (size_t)tg * lds, wb[tg], true, n, 32 * bi, 32 * bj, nti, ntj, g);
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+              double an[4], bn[4];
+              if (s < 7) {
+                const int r = 4 * (s + 1) + tg;
+                h_frags(an, bn, buf + (size_t)r * lds, wb[r], true, n, 32 * bi, 32 * bj, nti, ntj, g);
+              }
+              h_mmas(acc, av, bv, nti, ntj, bi == bj);
+              if (s < 7) {
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                  av[a] = an[a];
+                  bv[a] = bn[a];
+                }
+              }
             }
           } else {
             for (int kk = 0; kk < rows; kk += 4) {
