@@ -209,9 +209,11 @@ int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const 
  * instances too large for shared memory) comes from a 1 MiB array that the
  * library keeps in device memory on every GPU that loads it, until the
  * process exits.  Problems whose qpb_workspace_size exceeds 1 MiB are
- * rejected with QPB_ERR_UNSUPPORTED; every problem whose instances fit in
- * shared memory (all n <= 32; up to about n = 64 when p = 2n) needs only
- * 256 bytes of it, for any batch size.
+ * rejected with QPB_ERR_UNSUPPORTED.  Problems planned with their instances
+ * in shared memory need only 256 bytes of it, for any batch size: all
+ * n <= 32 (FP64 and mixed), and mixed precision up to about n = 64 when
+ * p = 2n; FP64 instances with n > 32 run from global arenas (more of them
+ * stay resident per SM that way) and fit only in small batches.
  * Nothing is allocated, by this call or by the library on its behalf.  The
  * first call on a device looks up the array's device address (one-time
  * set-up), so make that first call before any stream capture.  All calls

@@ -297,9 +297,10 @@ QPB_DEV void diag_factor(const KKTView& f, int J0, int w, int real_end, int sign
   // in registers after full unrolling.
   double* col = st->col;
 #pragma unroll
-  // All 32 steps run: rows and columns beyond w are identity, so their steps
-  // change nothing (pivot 1, zero multipliers).
+  // Rows and columns beyond w are identity: the steps stop at w (a multiple
+  // of 8, the same for the whole warp).
   for (int k = 0; k < kPanel; ++k) {
+    if (k >= w) break;
     col[lane] = row[k];
     __syncwarp();
     // a reciprocal and a product: an FP64 division per lane is more than
@@ -488,6 +489,7 @@ QPB_NOINLINE void kkt_solve(const Team<NT>& t, const KKTView& f, double* v, Bloc
       for (int k = 0; k < kPanel; ++k) lrow[k] = (lane < w && k < lane) ? K[(size_t)(J0 + lane) * ld + J0 + k] : 0.0;
 #pragma unroll
       for (int k = 0; k < kPanel; ++k) {
+        if (k >= w) break;  // uniform: later steps touch no lane below w
         const double xk = __shfl_sync(kFull, x, k);
         if (k < lane) x = fma(-lrow[k], xk, x);
       }
@@ -538,6 +540,7 @@ QPB_NOINLINE void kkt_solve(const Team<NT>& t, const KKTView& f, double* v, Bloc
       for (int k = 0; k < kPanel; ++k) lcol[k] = (k < w && k > lane) ? K[(size_t)(J0 + k) * ld + J0 + lane] : 0.0;
 #pragma unroll
       for (int k = kPanel - 1; k >= 0; --k) {
+        if (k >= w) continue;  // uniform: those steps touch no lane below w
         const double xk = __shfl_sync(kFull, x, k);
         if (k > lane) x = fma(-lcol[k], xk, x);
       }

@@ -173,32 +173,44 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     teams = (int)(team_budget / arena);
     teams = teams > 8 ? 8 : teams;
   }
-  if (teams >= 1 && arena * teams <= team_budget) {
+  // The arena in shared memory, when it fits, unless (blocked FP64 path) an
+  // arena in global memory with G streamed through shared memory keeps more
+  // instances resident per SM: these kernels are latency-bound.
+  int per_sm_smem = 0;
+  if (teams >= 1 && arena * teams <= team_budget &&
+      occupancy(pl->fn, NT * teams, arena * teams, &per_sm_smem) != QPB_OK)
+    return QPB_ERR_CUDA;
+  int gstage = 0, per_sm_global = 0;
+  size_t gbytes = 0;
+  if (NT > 32 && d.n > 32 && d.p > 0 && !mixed) {
+    // stream G through shared memory in chunks of up to 32 rows
+    const int ldg = (d.n + 3) & ~3;
+    for (int rows = 32; rows >= 8; rows >>= 1) {
+      const size_t b = gstage_bytes(ldg, rows);
+      if (b <= team_budget) {
+        gstage = rows;
+        gbytes = b;
+        break;
+      }
+    }
+    if (gstage && occupancy(pl->fn, NT, gbytes, &per_sm_global) != QPB_OK) return QPB_ERR_CUDA;
+    if (per_sm_global > 4) per_sm_global = 4;
+  }
+  if (per_sm_smem >= 1 && per_sm_smem >= per_sm_global) {
     pl->in_smem = 1;
     pl->teams = teams;
     pl->smem_bytes = arena * teams;
   } else {
     pl->in_smem = 0;
     pl->teams = NT == 32 ? 4 : 1;
-    pl->smem_bytes = 0;
-    if (NT > 32 && d.p > 0 && !mixed) {
-      // stream G through shared memory in chunks of up to 32 rows
-      const int ldg = (d.n + 3) & ~3;
-      for (int rows = 32; rows >= 8; rows >>= 1) {
-        const size_t b = gstage_bytes(ldg, rows);
-        if (b <= team_budget) {
-          pl->gstage_rows = rows;
-          pl->smem_bytes = b;
-          break;
-        }
-      }
-    }
+    pl->smem_bytes = gbytes;
+    pl->gstage_rows = gstage;
   }
   pl->threads = NT * pl->teams;
   int per_sm = 0;
   if (occupancy(pl->fn, pl->threads, pl->smem_bytes, &per_sm) != QPB_OK) return QPB_ERR_CUDA;
   if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
-  if (!pl->in_smem && per_sm > 2) per_sm = 2;
+  if (!pl->in_smem && per_sm > 4) per_sm = 4;
   const long need = ((long)d.batch + pl->teams - 1) / pl->teams;
   long grid = (long)per_sm * di.sms;
   if (grid > need) grid = need;

@@ -57,25 +57,31 @@ struct Core {
   double* gbuf = nullptr;  // G chunk buffers in shared memory (arena in global memory), or none
   int gstage_rows = 0;
 
-  // FP64 factors: teams of one warp keep the split layout (L, Y, F) and
-  // per-column elimination; larger teams factor the whole KKT matrix blocked
-  // on the FP64 tensor cores (qpb_blocked.cuh).
+  // FP64 factors: teams of one warp, and instances with n <= 32, keep the
+  // split layout (L, Y, F) and per-column elimination (one panel's worth of
+  // work: the blocked pass's serial diagonal step would dominate); larger
+  // instances on larger teams factor the whole KKT matrix blocked on the
+  // FP64 tensor cores (qpb_blocked.cuh).
   static constexpr bool kBlocked = NT > 32;
+  QPB_DEV bool blocked() const { return kBlocked && n > kPanel; }
 
   QPB_DEV void reset_stats() { st_f32 = st_f64 = st_sweeps = st_flags = 0; use64 = 0; }
 
   QPB_NOINLINE void factor64() {
-    double r;
+    double r = 0.0;
+    bool done = false;
     if constexpr (kBlocked) {
-      const KKTView f = KKTRegion::view(c.fr.base, n, m);
-      form_kkt<NT>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w, gbuf, gstage_rows);
-      t.sync();
-      // the G chunk buffers are free again: they hold the factor's panels
-      const size_t pcap = gbuf ? (gstage_bytes(ld, gstage_rows) - 64) / sizeof(double) : 0;
-      r = kkt_factor<NT>(t, f, st, gbuf, pcap);
-    } else {
-      r = factor_kkt<NT, KC, double>(t, n, m, p, c.Q, c.G, c.A, ld, c.w, nullptr, c.fr.view<double>());
+      if (blocked()) {
+        const KKTView f = KKTRegion::view(c.fr.base, n, m);
+        form_kkt<NT>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w, gbuf, gstage_rows);
+        t.sync();
+        // the G chunk buffers are free again: they hold the factor's panels
+        const size_t pcap = gbuf ? (gstage_bytes(ld, gstage_rows) - 64) / sizeof(double) : 0;
+        r = kkt_factor<NT>(t, f, st, gbuf, pcap);
+        done = true;
+      }
     }
+    if (!done) r = factor_kkt<NT, KC, double>(t, n, m, p, c.Q, c.G, c.A, ld, c.w, nullptr, c.fr.view<double>());
     st_f64++;
     if (!(r < INFINITY)) st_flags |= kFlagBreakdown64;
   }
@@ -183,11 +189,13 @@ struct Core {
       }
     }
     if constexpr (kBlocked) {
-      reduced_blocked(rhs, v4, dx, dy);
-    } else {
-      if (t.warp() == 0) reduced_solve_warp<KC, double>(c.fr.view<double>(), n, m, rhs, v4, dx, dy, t.lane());
-      t.sync();
+      if (blocked()) {
+        reduced_blocked(rhs, v4, dx, dy);
+        return;
+      }
     }
+    if (t.warp() == 0) reduced_solve_warp<KC, double>(c.fr.view<double>(), n, m, rhs, v4, dx, dy, t.lane());
+    t.sync();
   }
 
   // min over the team's entries of -v/d for d < 0 (qpax/pdip.py:66-73 before the cap at 1).
