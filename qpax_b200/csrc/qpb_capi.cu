@@ -23,10 +23,14 @@ int chunks_for(int k) {
   return c <= 1 ? 1 : c <= 2 ? 2 : c <= 4 ? 4 : 8;
 }
 
-static int auto_team(int n, int KC) {
-  if (KC >= 8) return 256;
-  if (KC >= 4) return n > 96 ? 256 : 128;
-  if (n <= 16) return 32;
+// Threads per instance.  FP64: 128 (four warps saturate the FP64 tensor
+// pipe; several instances share an SM and hide each other's serial steps).
+// Mixed keeps the per-column FP32 factorisation, which wants more threads
+// for large n.
+static int auto_team(int n, int KC, bool mixed) {
+  if (n <= 16 && KC == 1) return 32;
+  if (mixed && KC >= 8) return 256;
+  if (mixed && KC >= 4) return n > 96 ? 256 : 128;
   return 128;
 }
 
@@ -152,9 +156,8 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     return QPB_OK;
   }
   const int KC = chunks_for(d.n > d.m ? d.n : d.m);
-  int NT = cfg.team_threads ? cfg.team_threads : auto_team(d.n, KC);
+  int NT = cfg.team_threads ? cfg.team_threads : auto_team(d.n, KC, mixed);
   if (NT == 32 && KC > 1) NT = 128;
-  if (NT == 128 && KC > 4) NT = 256;
   if (NT == 256 && KC < 4) NT = 128;
   KernelFn fn = pick_kernel(elastic, mixed, NT, KC);
   if (!fn) return QPB_ERR_UNSUPPORTED;
@@ -183,18 +186,21 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   int gstage = 0, per_sm_global = 0;
   size_t gbytes = 0;
   if (NT > 32 && d.n > 32 && d.p > 0 && !mixed) {
-    // stream G through shared memory in chunks of up to 32 rows
+    // stream G through shared memory in chunks of 32, 16 or 8 rows: the
+    // largest chunk among those that keep the most instances per SM
     const int ldg = (d.n + 3) & ~3;
     for (int rows = 32; rows >= 8; rows >>= 1) {
       const size_t b = gstage_bytes(ldg, rows);
-      if (b <= team_budget) {
+      if (b > team_budget) continue;
+      int v = 0;
+      if (occupancy(pl->fn, NT, b, &v) != QPB_OK) return QPB_ERR_CUDA;
+      if (v > 4) v = 4;
+      if (v > per_sm_global) {
+        per_sm_global = v;
         gstage = rows;
         gbytes = b;
-        break;
       }
     }
-    if (gstage && occupancy(pl->fn, NT, gbytes, &per_sm_global) != QPB_OK) return QPB_ERR_CUDA;
-    if (per_sm_global > 4) per_sm_global = 4;
   }
   if (per_sm_smem >= 1 && per_sm_smem >= per_sm_global) {
     pl->in_smem = 1;

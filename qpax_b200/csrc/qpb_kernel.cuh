@@ -67,7 +67,7 @@ KernelFn kernel_warp_f64(int NP);
 constexpr int kWarpKernelThreads = 128;
 
 // (NT, KC) variants compiled into the library.
-#define QPB_FOR_EACH_VARIANT(X) X(32, 1) X(128, 1) X(128, 2) X(128, 4) X(256, 4) X(256, 8)
+#define QPB_FOR_EACH_VARIANT(X) X(32, 1) X(128, 1) X(128, 2) X(128, 4) X(128, 8) X(256, 4) X(256, 8)
 
 
 }  // namespace qpb
