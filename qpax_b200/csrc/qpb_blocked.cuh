@@ -161,6 +161,32 @@ QPB_DEV void h_block_kstep(double (&acc)[4][4][2], const double* row, double wk,
   h_mmas(acc, av, bv, nti, ntj, diag);
 }
 
+// A full chunk of kRows staged rows: the next k-step's fragments load under
+// this one's MMAs.
+template <int kRows>
+QPB_DEV void h_chunk_pipelined(double (&acc)[4][4][2], const double* buf, const double* wb, int lds, int n, int bi,
+                               int bj, int nti, int ntj, int g, int tg) {
+  constexpr int kSteps = kRows / 4;
+  double av[4], bv[4];
+  h_frags(av, bv, buf + (size_t)tg * lds, wb[tg], true, n, 32 * bi, 32 * bj, nti, ntj, g);
+#pragma unroll
+  for (int s = 0; s < kSteps; ++s) {
+    double an[4], bn[4];
+    if (s + 1 < kSteps) {
+      const int r = 4 * (s + 1) + tg;
+      h_frags(an, bn, buf + (size_t)r * lds, wb[r], true, n, 32 * bi, 32 * bj, nti, ntj, g);
+    }
+    h_mmas(acc, av, bv, nti, ntj, bi == bj);
+    if (s + 1 < kSteps) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        av[a] = an[a];
+        bv[a] = bn[a];
+      }
+    }
+  }
+}
+
 // K <- [sym(Q) + G' diag(w) G, A'; A, 0] (lower triangle, padded).  G, A, Q
 // are row-major with leading dimensions ldg, lda, ldq (ldg a multiple of 4);
 // rows of G beyond p and columns beyond n read as zero.  H is computed in
@@ -183,7 +209,10 @@ QPB_NOINLINE void form_kkt(const Team<NT>& t, const KKTView& f, int p, const dou
       tri_pair(tau, bi, bj);
       const int nti = min(4, (n8 - 32 * bi) >> 3), ntj = min(4, (n8 - 32 * bj) >> 3);
       double acc[4][4][2] = {};
-      for (int k0 = 0; k0 < p; k0 += 4) {
+      int k0 = 0;
+      for (; k0 + 32 <= p; k0 += 32)  // whole 32-row groups, pipelined
+        h_chunk_pipelined<32>(acc, G + (size_t)k0 * ldg, wv + k0, ldg, n, bi, bj, nti, ntj, g, tg);
+      for (; k0 < p; k0 += 4) {
         const int k = k0 + tg;
         const bool in = k < p;
         h_block_kstep(acc, G + (size_t)(in ? k : 0) * ldg, in ? wv[k] : 0.0, in, n, 32 * bi, 32 * bj, nti, ntj,
@@ -228,26 +257,12 @@ QPB_NOINLINE void form_kkt(const Team<NT>& t, const KKTView& f, int p, const dou
           const double* buf = gbuf + (size_t)(ch & 1) * KR * lds;
           const double* wb = wbuf + (ch & 1) * KR;
           const int rows = min(KR, p - ch * KR);
-          if (rows == 32 && KR == 32) {
-            // full chunk: the next k-step's fragments load under this one's MMAs
-            double av[4], bv[4];
-            h_frags(av, bv, buf + (size_t)tg * lds, wb[tg], true, n, 32 * bi, 32 * bj, nti, ntj, g);
-#pragma unroll
-            for (int s = 0; s < 8; ++s) {
-              double an[4], bn[4];
-              if (s < 7) {
-                const int r = 4 * (s + 1) + tg;
-                h_frags(an, bn, buf + (size_t)r * lds, wb[r], true, n, 32 * bi, 32 * bj, nti, ntj, g);
-              }
-              h_mmas(acc, av, bv, nti, ntj, bi == bj);
-              if (s < 7) {
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                  av[a] = an[a];
-                  bv[a] = bn[a];
-                }
-              }
-            }
+          if (rows == KR && KR == 32) {
+            h_chunk_pipelined<32>(acc, buf, wb, lds, n, bi, bj, nti, ntj, g, tg);
+          } else if (rows == KR && KR == 16) {
+            h_chunk_pipelined<16>(acc, buf, wb, lds, n, bi, bj, nti, ntj, g, tg);
+          } else if (rows == KR && KR == 8) {
+            h_chunk_pipelined<8>(acc, buf, wb, lds, n, bi, bj, nti, ntj, g, tg);
           } else {
             for (int kk = 0; kk < rows; kk += 4) {
               const int r = kk + tg;
