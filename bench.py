@@ -11,7 +11,7 @@ Inputs are resident in HBM; L2 is flushed (256 MB write) between steps,
 outside the per-step CUDA events.  Synthetic seeded data (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload dense|nnls|small|uneven|elastic]
+                    [--workload dense|nnls|small|uneven|elastic] [--batch B]
 
 Other workloads (same JSON line, `config.workload` names them):
   nnls     10000 non-negative least squares QPs, n = 5, G = -I, no equalities
@@ -197,22 +197,16 @@ def dist_setup(gpus):
 
 
 def barrier_max(val, world):
-    import torch
+    from qpax_b200.shard import max_over_ranks
 
-    if world == 1:
-        return val
-    import torch.distributed as dist
-
-    t = torch.tensor([val], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return max_over_ranks(val) if world > 1 else val
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from qpax_b200.shard import barrier as _barrier
 
-        dist.barrier()
+    if world > 1:
+        _barrier()
 
 
 # ------------------------------------------------------------- CPU (oracle)
@@ -681,12 +675,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dense")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instances per GPU (default: the workload's own); smaller batches are for profiling")
     ap.add_argument("--only-default", action="store_true", help="time only the default (auto) path")
     ap.add_argument("--e2e-chunks", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
+    if args.batch > 0 and args.batch != spec.batch:
+        spec = Spec(spec.key, spec.kind, args.batch, spec.n, spec.m, spec.p, spec.tol,
+                    spec.workload.replace(f"{spec.batch}", f"{args.batch}", 1))
     if args.impl == "reference":
         # host-only: rank 0 times the CPU implementation, other ranks exit
         world = int(os.environ.get("WORLD_SIZE", "1"))
