@@ -49,6 +49,9 @@ struct ElasticArena : CoreArena {
 
 template <int NT, int KC, bool kMixed>
 struct ElasticQP {
+  // CTAs per SM the register budget is cut for (128-thread teams): three
+  // (at four, 128 registers, the elastic steps spill and run slower).
+  static constexpr int kMinBlocks = NT == 128 ? 3 : 1;
   Core<NT, KC, kMixed> k;
   ElasticArena a;
   const Params* P;

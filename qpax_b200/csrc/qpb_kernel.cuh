@@ -7,15 +7,14 @@
 namespace qpb {
 
 // Register budget: blocks of up to 256 threads; 128-thread teams are held to
-// 128 registers so that four instances fit on an SM (these kernels are
+// the solver's kMinBlocks resident CTAs per SM (these kernels are
 // latency-bound: resident instances hide each other's serial steps).
-constexpr int kipm_min_blocks(int NT) { return NT == 128 ? 3 : 1; }
 constexpr int kipm_max_threads(int NT) { return NT == 128 ? 128 : 256; }
 
 // Persistent: each team pulls instance indices from P.counter until the
 // batch is exhausted (a bounded loop: at most `batch` fetches in total).
 template <class Solver, int NT>
-__global__ void __launch_bounds__(kipm_max_threads(NT), kipm_min_blocks(NT)) ipm_kernel(const __grid_constant__ Params P) {
+__global__ void __launch_bounds__(kipm_max_threads(NT), Solver::kMinBlocks) ipm_kernel(const __grid_constant__ Params P) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int next_inst;
   const int teams = blockDim.x / NT;
