@@ -137,6 +137,50 @@ def test_larger_instances(prec, n):
         assert_close(np_(g)[ok], go[ok], G_TOL, name)
 
 
+# Shapes that reach every branch of the blocked FP64 KKT factorisation
+# (n > 32): n and m off multiples of 8 (partial panels, identity pads), no
+# equalities (no Schur phase), a Schur complement wider than one panel, tiny p
+# (the arena then stays in shared memory), the largest shapes (global arenas,
+# G staged through shared memory, staged factor panels), p = 0 (qpax's
+# equality-only exit).
+BLOCKED_SHAPES = [(33, 0, 66), (37, 9, 20), (45, 40, 90), (70, 3, 4), (256, 64, 512), (40, 10, 0)]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", BLOCKED_SHAPES)
+def test_blocked_factorisation_shapes(prec, shape):
+    n, m, p = shape
+    B = 3 if n > 128 else 8
+    Q, q, A, b, G, h = wl.dense(B, n, m, p, 300 + n + m + p)
+    _, ref = check_solve(Q, q, A, b, G, h, 1e-6, prec, max_breakdown=0.5)
+    if p == 0:
+        return  # qpax's relax / VJP need inequalities
+    ok = ref[4] == 1
+    (_, grads, _, _), (_, grads_o, _, _) = _vjp_pair(Q, q, A, b, G, h, 1e-6, 1e-3, prec)
+    for g, go, name in zip(grads, grads_o, ["dQ", "dq", "dA", "db", "dG", "dh"]):
+        assert_close(np_(g)[ok], go[ok], G_TOL, name)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_elastic_blocked_global_arena(prec):
+    """Elastic QPs large enough for the blocked factorisation from a global
+    arena (n = 100, p = 150): x and the slacks vs the oracle.  With the
+    penalty at 1e3 the final residual of some instances lands next to the
+    tolerance, where LDL' (here) and QR (qpax) rounding can decide the last
+    iteration differently: counts may differ by one; the outputs must agree."""
+    import qpax_b200 as qb
+
+    Q, q, G, h, _ = wl.elastic(6, seed=77, n=100, p=150)
+    out = qb.solve_qp_elastic(Q, q, G, h, 1e3, 1e-6, **VARIANTS[prec])
+    ref = oracle.solve_qp_elastic(Q, q, G, h, 1e3, solver_tol=1e-6)
+    ok = ref[6] == 1
+    assert ok.any()
+    np.testing.assert_array_equal(np_(out[6])[ok], 1)
+    assert np.abs(np_(out[7])[ok].astype(int) - ref[7][ok]).max() <= 1
+    for k, name in enumerate(["x", "t", "s1", "s2"]):
+        assert_close(np_(out[k])[ok], ref[k][ok], X_TOL, name)
+
+
 def test_autograd_matches_vjp():
     """torch.autograd through solve_qp_primal equals the explicit VJP."""
     import qpax_b200 as qb
