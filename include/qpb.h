@@ -225,6 +225,27 @@ int qpb_solve_qp_noalloc(const qpb_dims* dims, const double* Q, const double* q,
                          double* s, double* z, double* y, int32_t* converged, int32_t* iters,
                          const qpb_config* cfg, qpb_stream_t stream);
 
+/* Forward and backward of qpax/diff_qp.py:49-82 solve_qp_primal (qpb_solve_qp,
+ * then qpb_solve_qp_primal_bwd) on a batch held in HOST memory -- the call a
+ * qpax user with NumPy / CPU arrays makes.  The batch is cut into `chunks`
+ * slices; each slice is copied in, solved forward and backward, and its x,
+ * six gradients and (optional) converged / iters are copied out, on three
+ * internal streams so that copies of one slice overlap the kernels of
+ * another.  Q..h, dl_dx, x, dQ..dh, converged, iters are HOST pointers (pin
+ * them -- cudaHostAlloc / cudaHostRegister -- for the copies to overlap);
+ * converged and iters may be NULL.  `workspace` is DEVICE memory of
+ * qpb_solve_qp_primal_vjp_host_workspace_size bytes (256-byte aligned).
+ * Everything is enqueued after the work already on `stream`, and `stream`
+ * waits for all of it: synchronize `stream` before reading the outputs.
+ * Requires p >= 1. */
+size_t qpb_solve_qp_primal_vjp_host_workspace_size(const qpb_dims* dims, int32_t chunks, const qpb_config* cfg);
+int qpb_solve_qp_primal_vjp_host(const qpb_dims* dims, const double* Q, const double* q, const double* A,
+                                 const double* b, const double* G, const double* h, const double* dl_dx,
+                                 double solver_tol, double target_kappa, double* x, double* dQ, double* dq,
+                                 double* dA, double* db, double* dG, double* dh, int32_t* converged, int32_t* iters,
+                                 int32_t chunks, const qpb_config* cfg, void* workspace, size_t workspace_bytes,
+                                 qpb_stream_t stream);
+
 /* Human-readable name of a qpb_status code. */
 const char* qpb_status_string(int status);
 

@@ -56,10 +56,11 @@ _SIGS = {
     "qpb_relax_qp_elastic": "dims P P P P P A6 D D A6 P P cfg P S stream",
     "qpb_diff_qp_elastic": "dims P P P P P A6 P P P P P cfg P S stream",
     "qpb_solve_qp_elastic_primal_bwd": "dims P P P P P A6 P D D P P P P cfg P S stream",
+    "qpb_solve_qp_primal_vjp_host": "dims P P P P P P P D D P P P P P P P P P I cfg P S stream",
 }
 _CT = {
     "dims": ctypes.POINTER(Dims), "cfg": ctypes.POINTER(Config), "P": ctypes.c_void_p, "D": ctypes.c_double,
-    "S": ctypes.c_size_t, "stream": ctypes.c_void_p, "A6": ctypes.POINTER(ctypes.c_void_p),
+    "S": ctypes.c_size_t, "stream": ctypes.c_void_p, "A6": ctypes.POINTER(ctypes.c_void_p), "I": ctypes.c_int32,
 }
 
 
@@ -77,6 +78,9 @@ def load() -> ctypes.CDLL:
                 fn.restype = ctypes.c_int
             lib.qpb_workspace_size.argtypes = [ctypes.c_int32, ctypes.POINTER(Dims), ctypes.POINTER(Config)]
             lib.qpb_workspace_size.restype = ctypes.c_size_t
+            lib.qpb_solve_qp_primal_vjp_host_workspace_size.argtypes = [ctypes.POINTER(Dims), ctypes.c_int32,
+                                                                        ctypes.POINTER(Config)]
+            lib.qpb_solve_qp_primal_vjp_host_workspace_size.restype = ctypes.c_size_t
             lib.qpb_status_string.argtypes = [ctypes.c_int]
             lib.qpb_status_string.restype = ctypes.c_char_p
             lib.qpb_version.restype = ctypes.c_int32
@@ -85,7 +89,8 @@ def load() -> ctypes.CDLL:
 
 
 def exported_symbols() -> list[str]:
-    return ["qpb_workspace_size", "qpb_status_string", "qpb_version"] + list(_SIGS)
+    return ["qpb_workspace_size", "qpb_status_string", "qpb_version",
+            "qpb_solve_qp_primal_vjp_host_workspace_size"] + list(_SIGS)
 
 
 def device() -> torch.device:

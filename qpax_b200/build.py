@@ -32,6 +32,7 @@ SOURCES = [
     "qpb_bench.cu",
     "qpb_noalloc.cu",
     "qpb_plan.cu",
+    "qpb_host_pipeline.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE]

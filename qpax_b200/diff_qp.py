@@ -77,55 +77,54 @@ def diff_qp(Q, q, A, b, G, h, x, s, lam, nu, dl_dx, *, precision=None, team_thre
     return bt.out(dQ, dq, dA, db, dG, dh)
 
 
-_STREAMS: dict = {}
+_HOST_WS: dict = {}
 
 
-def _host_streams(dev, count):
-    """Streams of the host pipeline, created once per device and reused (new
-    streams per call would defeat the caching allocator's per-stream reuse)."""
-    key = (dev.index, count)
-    if key not in _STREAMS:
-        _STREAMS[key] = [torch.cuda.Stream(device=dev) for _ in range(count)]
-    return _STREAMS[key]
+def _host_workspace(dev, nbytes):
+    """Device workspace of the host-buffer pipeline, kept per device and grown
+    on demand (allocating per call would serialize on the allocator)."""
+    ws = _HOST_WS.get(dev.index)
+    if ws is None or ws.numel() < nbytes + 256:
+        ws = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+        _HOST_WS[dev.index] = ws
+    return ws
 
 
 def solve_qp_primal_vjp_host(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, target_kappa: float = 1e-3, *,
-                             out=None, chunks: int = 4, streams: int = 3, precision=None):
+                             out=None, chunks: int = 4, precision=None, team_threads=None):
     """solve_qp_primal_vjp for batches that live in host memory.
 
-    Inputs are CPU tensors with a leading batch axis (pinned memory lets the
-    copies overlap); the batch is cut into `chunks`, and on `streams` CUDA
-    streams each chunk is copied in, solved forward and backward, and its x
-    and six gradients copied back while the next chunk computes.  `out` may
-    hold preallocated pinned CPU tensors (x, dQ, dq, dA, db, dG, dh).
+    Inputs are CPU float64 tensors (or arrays) with a leading batch axis;
+    pinned memory lets the copies overlap the kernels.  One call of
+    qpb_solve_qp_primal_vjp_host: the batch is cut into `chunks`, and each
+    chunk is copied in, solved forward and backward, and its x and six
+    gradients copied back while other chunks compute.  `out` may hold
+    preallocated (pinned) CPU tensors (x, dQ, dq, dA, db, dG, dh).
     Returns (x, (dQ, dq, dA, db, dG, dh)) on the host; waits for completion.
     """
     dev = _lib.device()
-    B = Q.shape[0]
+    ins = [torch.as_tensor(t, dtype=torch.float64) for t in (Q, q, A, b, G, h, dl_dx)]
+    if any(t.device.type != "cpu" for t in ins):
+        raise ValueError("solve_qp_primal_vjp_host takes host (CPU) tensors")
+    ins = [t.contiguous() for t in ins]
+    Qh, qh, Ah, bh, Gh, hh, gh = ins
+    B, n, m, p = Qh.shape[0], Qh.shape[-1], Ah.shape[-2], Gh.shape[-2]
     if out is None:
         pin = torch.cuda.is_available()
-        out = [torch.empty(t.shape, dtype=torch.float64, pin_memory=pin) for t in (q, Q, q, A, b, G, h)]
-    bounds = [round(i * B / chunks) for i in range(chunks + 1)]
-    pool = _host_streams(dev, max(1, streams))
-    main = torch.cuda.current_stream(dev)
-    for s in pool:
-        s.wait_stream(main)
-    opts = dict(precision=precision)
-    for c in range(chunks):
-        lo, hi = bounds[c], bounds[c + 1]
-        if hi <= lo:
-            continue
-        s = pool[c % len(pool)]
-        with torch.cuda.stream(s):
-            dev_in = [t[lo:hi].to(dev, non_blocking=True) for t in (Q, q, A, b, G, h, dl_dx)]
-            x, grads, _, _ = solve_qp_primal_vjp(*dev_in[:6], dev_in[6], solver_tol, target_kappa, **opts)
-            for dst, src in zip(out, (x,) + tuple(grads)):
-                dst[lo:hi].copy_(src, non_blocking=True)
-            for t in dev_in:
-                t.record_stream(s)
-    for s in pool:
-        main.wait_stream(s)
-    torch.cuda.synchronize(dev)
+        out = [torch.empty(t.shape, dtype=torch.float64, pin_memory=pin) for t in (qh, Qh, qh, Ah, bh, Gh, hh)]
+    dims = _lib.Dims(B, n, m, p)
+    cfg = _config(dict(precision=precision, team_threads=team_threads))
+    lib = _lib.load()
+    chunks = max(1, min(int(chunks), max(B, 1)))
+    need = lib.qpb_solve_qp_primal_vjp_host_workspace_size(ctypes.byref(dims), chunks, ctypes.byref(cfg))
+    if need == 0:
+        raise _lib.QpbError(f"unsupported problem for the host pipeline: batch={B} n={n} m={m} p={p}")
+    wp, wb = _lib.aligned(_host_workspace(dev, need))
+    stream = torch.cuda.current_stream(dev)
+    _lib.call("qpb_solve_qp_primal_vjp_host", ctypes.byref(dims), *[ptr(t) for t in ins],
+              ctypes.c_double(solver_tol), ctypes.c_double(target_kappa), *[ptr(t) for t in out], None, None,
+              chunks, ctypes.byref(cfg), wp, wb, stream.cuda_stream)
+    stream.synchronize()
     return out[0], tuple(out[1:])
 
 

@@ -181,6 +181,23 @@ def test_elastic_blocked_global_arena(prec):
         assert_close(np_(out[k])[ok], ref[k][ok], X_TOL, name)
 
 
+@pytest.mark.parametrize("shape,chunks", [((32, 8, 64), 3), ((40, 0, 80), 1), ((12, 3, 24), 5)])
+def test_host_buffer_pipeline(shape, chunks):
+    """qpb_solve_qp_primal_vjp_host (host arrays in, host arrays out, chunked
+    and overlapped) gives exactly what the device-resident calls give."""
+    import qpax_b200 as qb
+
+    n, m, p = shape
+    data = wl.dense(23, n, m, p, 500 + n)
+    dl = np.full((23, n), 0.1)
+    x_h, g_h = qb.solve_qp_primal_vjp_host(*[torch.tensor(a).pin_memory() for a in data],
+                                           torch.tensor(dl).pin_memory(), 1e-6, 1e-3, chunks=chunks)
+    x_d, g_d, _, _ = qb.solve_qp_primal_vjp(*data, dl, 1e-6, 1e-3)
+    np.testing.assert_array_equal(x_h.numpy(), np_(x_d))
+    for a, b_, name in zip(g_h, g_d, ["dQ", "dq", "dA", "db", "dG", "dh"]):
+        np.testing.assert_array_equal(a.numpy(), np_(b_), err_msg=name)
+
+
 def test_autograd_matches_vjp():
     """torch.autograd through solve_qp_primal equals the explicit VJP."""
     import qpax_b200 as qb
