@@ -130,6 +130,14 @@ int qpb_plan_create(qpb_plan** out, int32_t batch, const int32_t* shapes, const 
     }
     b.count = (int)(list.size() - b.list_off);
     b.work = work;
+    // heaviest instances first: the persistent teams pull them in list
+    // order, so the launch ends on light instances instead of a long tail
+    auto inst_work = [&](int32_t i) {
+      const double n = shapes[3 * i], m = shapes[3 * i + 1], p = shapes[3 * i + 2];
+      return p * n * n + n * n * n / 3.0 + 2.0 * m * n * n;
+    };
+    std::stable_sort(list.begin() + b.list_off, list.end(),
+                     [&](int32_t x, int32_t y) { return inst_work(x) > inst_work(y); });
     const qpb_dims dm{b.count, b.n_max, b.m_max, b.p_max};
     // size the launch for the largest member; the backward op needs the same arena
     int st = make_plan(kOpSolve, dm, c, &b.launch);
