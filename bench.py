@@ -637,9 +637,11 @@ def run_e2e(args, spec: Spec, data, dev, arm):
 
         path = "qpax_b200.solve_qp_elastic_primal_vjp (C ABI): pinned host tensors copied in and out on one stream"
     else:
-        from qpax_b200.packed import pack
+        from qpax_b200.packed import PackedHostPipeline, pack
 
         plan = arm.plan
+        n_, m_, p_ = shapes_of(spec, data)
+        pipe = PackedHostPipeline(list(zip(n_, m_, p_)), chunks=args.e2e_chunks)
         host = [pack(v, torch.device("cpu")).pin_memory() for v in data]
         g_host = torch.full((plan.totals[1],), 0.1, dtype=torch.float64).pin_memory()
         outs_host = [torch.empty(plan.totals[1], dtype=torch.float64).pin_memory()] + \
@@ -648,13 +650,10 @@ def run_e2e(args, spec: Spec, data, dev, arm):
         d2h = sum(t.numel() * 8 for t in outs_host)
 
         def step():
-            d = [t.to(dev, non_blocking=True) for t in host + [g_host]]
-            out = plan.solve(*d[:6], spec.tol)
-            grads = plan.primal_bwd(*d[:6], *out[:4], d[6], spec.tol, KAPPA)
-            for dst, src in zip(outs_host, (out[0],) + tuple(grads)):
-                dst.copy_(src, non_blocking=True)
+            pipe.run(*host, g_host, spec.tol, KAPPA, out=outs_host)
 
-        path = "qpax_b200.PackedPlan (C ABI plan): packed pinned host tensors copied in and out on one stream"
+        path = (f"qpax_b200.packed.PackedHostPipeline (C ABI plans): packed pinned host tensors, {args.e2e_chunks} "
+                "instance groups over 3 streams (copy in / solve + backward / copy out overlap)")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

@@ -142,3 +142,70 @@ def solve_qp_uneven(Qs, qs, As, bs, Gs, hs, solver_tol: float = 1e-3, precision:
     x, s, z, y, conv, iters = plan.solve(*ins, solver_tol)
     L = plan.lengths
     return unpack(x, L[1]), unpack(s, L[5]), unpack(z, L[5]), unpack(y, L[3]), conv, iters
+
+
+class PackedHostPipeline:
+    """Forward + backward of solve_qp_primal on an uneven batch held in host
+    memory, with copies overlapped with the kernels.
+
+    The instances are cut into `chunks` contiguous groups (contiguous in every
+    packed array), each with its own plan and device buffers; on three
+    streams each group is copied in, solved forward and backward, and its x and
+    six gradients copied back while the other groups compute.
+
+        pipe = PackedHostPipeline(shapes, chunks=4)
+        x, grads = pipe.run(Q, q, A, b, G, h, dl_dx, solver_tol, target_kappa, out=None)
+
+    Inputs are packed 1-D CPU float64 tensors (pinned for the copies to
+    overlap); `out` may hold packed CPU tensors (x, dQ, dq, dA, db, dG, dh).
+    """
+
+    def __init__(self, shapes, chunks: int = 4, precision: str = "auto", streams: int = 3):
+        sh = np.ascontiguousarray(np.asarray(shapes, dtype=np.int32).reshape(-1, 3))
+        B = sh.shape[0]
+        chunks = max(1, min(int(chunks), B))
+        self.bounds = [B * c // chunks for c in range(chunks + 1)]
+        self.lengths = sizes(sh)
+        self.totals = [int(np.sum(v)) for v in self.lengths]
+        # element offset of instance i in each packed field
+        self.offs = [np.concatenate([[0], np.cumsum(v)]) for v in self.lengths]
+        self.plans = [PackedPlan(sh[lo:hi], precision) for lo, hi in zip(self.bounds[:-1], self.bounds[1:])]
+        self.dev = _lib.device()
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(max(1, streams))]
+        # field of each input / output: Q q A b G h dl -> 0 1 2 3 4 5 1; x dQ dq dA db dG dh -> 1 0 1 2 3 4 5
+        self.in_fields = [0, 1, 2, 3, 4, 5, 1]
+        self.out_fields = [1, 0, 1, 2, 3, 4, 5]
+        self.dev_in = [[torch.empty(p.totals[k], dtype=torch.float64, device=self.dev) for k in self.in_fields]
+                       for p in self.plans]
+
+    def _span(self, field, c):
+        lo, hi = self.bounds[c], self.bounds[c + 1]
+        return int(self.offs[field][lo]), int(self.offs[field][hi])
+
+    def run(self, Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, target_kappa: float = 1e-3, out=None):
+        host_in = [torch.as_tensor(t, dtype=torch.float64).reshape(-1) for t in (Q, q, A, b, G, h, dl_dx)]
+        if out is None:
+            pin = torch.cuda.is_available()
+            out = [torch.empty(self.totals[f], dtype=torch.float64, pin_memory=pin) for f in self.out_fields]
+        main = torch.cuda.current_stream(self.dev)
+        for s in self.streams:
+            s.wait_stream(main)
+        for c, plan in enumerate(self.plans):
+            s = self.streams[c % len(self.streams)]
+            with torch.cuda.stream(s):
+                d = self.dev_in[c]
+                for dst, src, f in zip(d, host_in, self.in_fields):
+                    lo, hi = self._span(f, c)
+                    dst.copy_(src[lo:hi], non_blocking=True)
+                res = plan.solve(*d[:6], solver_tol)
+                grads = plan.primal_bwd(*d[:6], *res[:4], d[6], solver_tol, target_kappa)
+                for dst, src, f in zip(out, (res[0],) + tuple(grads), self.out_fields):
+                    lo, hi = self._span(f, c)
+                    dst[lo:hi].copy_(src, non_blocking=True)
+                    src.record_stream(s)
+                for t in res:
+                    t.record_stream(s)
+        for s in self.streams:
+            main.wait_stream(s)
+        torch.cuda.synchronize(self.dev)
+        return out[0], tuple(out[1:])
