@@ -293,9 +293,9 @@ QPB_NOINLINE void form_kkt(const Team<NT>& t, const KKTView& f, int p, const dou
 
 // LDL' of the w x w diagonal block at (J0, J0) by one warp: lane r owns row r
 // (entries c <= r in registers), pivot columns are broadcast through shared
-// memory.  Writes
-// the unit factor and the pivots to K, 1/d to dinv, and a copy to the stage.
-// Pivots of rows J0 + r < real_end are checked (must be positive, finite).
+// memory.  Writes the unit factor and the pivots to K, 1/d to dinv, and a
+// copy to the stage.  Pivots of rows J0 + r < real_end are checked (must be
+// positive and finite).
 QPB_DEV void diag_factor(const KKTView& f, int J0, int w, int real_end, int sign, BlockedStage* st, int lane,
                          double& dmin, double& dmax, int& bad) {
   double* K = f.K;
@@ -309,11 +309,10 @@ QPB_DEV void diag_factor(const KKTView& f, int J0, int w, int real_end, int sign
   }
   // Column k is broadcast through shared memory (every lane stores its entry
   // k, then reads the others): unlike a shuffle per entry, this keeps `row`
-  // in registers after full unrolling.
+  // in registers after full unrolling.  Rows and columns beyond w are
+  // identity: the steps stop at w (a multiple of 8, the same for the warp).
   double* col = st->col;
 #pragma unroll
-  // Rows and columns beyond w are identity: the steps stop at w (a multiple
-  // of 8, the same for the whole warp).
   for (int k = 0; k < kPanel; ++k) {
     if (k >= w) break;
     col[lane] = row[k];
