@@ -89,3 +89,24 @@ def test_api_refuses_to_run_without_a_device():
 
     with pytest.raises(QpbError):
         qb.solve_qp([[1.0]], [1.0], [[0.0]][:0], [], [[1.0]], [1.0])
+
+
+def test_host_pipeline_rejects_bad_arguments(lib):
+    """qpb_solve_qp_primal_vjp_host checks its arguments on the host before any
+    copy or launch."""
+    from qpax_b200._lib import Dims
+
+    def call(dims, chunks=2, **over):
+        names = ["Q", "q", "A", "b", "G", "h", "dl", "x", "dQ", "dq", "dA", "db", "dG", "dh"]
+        ptrs = [over.get(k, 8) for k in names]
+        d = ctypes.byref(dims) if dims is not None else None
+        return lib.qpb_solve_qp_primal_vjp_host(d, *ptrs[:7], ctypes.c_double(1e-5), ctypes.c_double(1e-3),
+                                                *ptrs[7:], None, None, chunks, None, 256, 1 << 20, None)
+
+    assert call(None) == 1                              # null dims
+    assert call(Dims(4, 3, 1, 2), chunks=0) == 1        # no chunks
+    assert call(Dims(4, 3, 1, 0)) == 2                  # qpax's relax / VJP need inequalities
+    assert call(Dims(4, 3, 1, 2), G=None) == 1          # missing input
+    assert call(Dims(4, 3, 1, 2), dG=12) == 1           # misaligned output
+    assert call(Dims(0, 3, 1, 2)) == 0                  # empty batch: nothing to do
+    assert lib.qpb_solve_qp_primal_vjp_host_workspace_size(ctypes.byref(Dims(4, 3, 1, 2)), 0, None) == 0
