@@ -678,11 +678,16 @@ def main():
     ap.add_argument("--batch", type=int, default=0,
                     help="instances per GPU (default: the workload's own); smaller batches are for profiling")
     ap.add_argument("--only-default", action="store_true", help="time only the default (auto) path")
-    ap.add_argument("--e2e-chunks", type=int, default=4)
+    ap.add_argument("--e2e-chunks", type=int, default=0,
+                    help="slices of the host-buffer pipeline (0: the workload's setting, measured best)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
+    if args.e2e_chunks <= 0:
+        # copies of the large workloads overlap best in 4-8 slices; small
+        # ones want few slices (each slice's launch must still fill the GPU)
+        args.e2e_chunks = {"dense": 4, "nnls": 2, "small": 2, "uneven": 8, "elastic": 1}[spec.key]
     if args.batch > 0 and args.batch != spec.batch:
         spec = Spec(spec.key, spec.kind, args.batch, spec.n, spec.m, spec.p, spec.tol,
                     spec.workload.replace(f"{spec.batch}", f"{args.batch}", 1))
