@@ -195,7 +195,10 @@ QPB_DEV void h_chunk_pipelined(double (&acc)[4][4][2], const double* buf, const 
 // through two chunk buffers of KR rows (cp.async double buffering), so each
 // row of G crosses from L2 once per round instead of once per block;
 // without it, fragments are read from G in place (G in shared memory).
-template <int NT>
+// kVariant only separates the compiled copies of the non-inlined phases per
+// kernel (its register budget differs between kernels; a shared copy would
+// be compiled for the smallest).
+template <int NT, int kVariant = 0>
 QPB_NOINLINE void form_kkt(const Team<NT>& t, const KKTView& f, int p, const double* Q, int ldq, const double* G,
                            int ldg, const double* A, int lda, const double* wv, double* gbuf, int KR) {
   constexpr int kWarps = NT / 32;
@@ -458,7 +461,7 @@ QPB_DEV void ldlt_phase(const Team<NT>& t, const KKTView& f, int J0s, int J0e, i
 
 // Factor K (already formed).  Returns the pivot ratio max(D)/min(D) of H, or
 // +inf when a pivot of H or of F is not strictly positive and finite.
-template <int NT>
+template <int NT, int kVariant = 0>
 QPB_NOINLINE double kkt_factor(const Team<NT>& t, const KKTView& f, BlockedStage* st, double* pbuf, size_t pcap) {
   double dmin = INFINITY, dmax = 0.0;
   int bad = 0;
@@ -487,7 +490,7 @@ QPB_NOINLINE double kkt_factor(const Team<NT>& t, const KKTView& f, BlockedStage
 }
 
 // v <- K^-1 v for the factored K (v: N entries in shared memory).
-template <int NT>
+template <int NT, int kVariant = 0>
 QPB_NOINLINE void kkt_solve(const Team<NT>& t, const KKTView& f, double* v, BlockedStage* st) {
   const double* K = f.K;
   const int ld = f.ld, N = f.N;

@@ -73,11 +73,11 @@ struct Core {
     if constexpr (kBlocked) {
       if (blocked()) {
         const KKTView f = KKTRegion::view(c.fr.base, n, m);
-        form_kkt<NT>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w, gbuf, gstage_rows);
+        form_kkt<NT, KC>(t, f, p, c.Q, ld, c.G, ld, c.A, ld, c.w, gbuf, gstage_rows);
         t.sync();
         // the G chunk buffers are free again: they hold the factor's panels
         const size_t pcap = gbuf ? (gstage_bytes(ld, gstage_rows) - 64) / sizeof(double) : 0;
-        r = kkt_factor<NT>(t, f, st, gbuf, pcap);
+        r = kkt_factor<NT, KC>(t, f, st, gbuf, pcap);
         done = true;
       }
     }
@@ -99,7 +99,7 @@ struct Core {
       v[i] = x;
     }
     t.sync();
-    kkt_solve<NT>(t, f, v, st);
+    kkt_solve<NT, KC>(t, f, v, st);
     for (int i = t.r; i < n; i += NT) dx[i] = v[i];
     for (int i = t.r; i < m; i += NT) dy[i] = v[f.n8 + i];
     t.sync();
