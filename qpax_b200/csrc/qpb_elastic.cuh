@@ -78,29 +78,14 @@ struct ElasticQP {
     const Team<NT>& tm = T();
     const double* gQ = P->Q + inst * (long)n * n;
     const double* gG = P->G + inst * (long)p * n;
-    for (int e = tm.r; e < n * ld; e += NT) {
-      const int i = e / ld, j = e - i * ld;
-      a.Q[e] = (j < n) ? gQ[(long)i * n + j] : 0.0;
-    }
-    for (int e = tm.r; e < p * ld; e += NT) {
-      const int i = e / ld, j = e - i * ld;
-      a.G[e] = (j < n) ? gG[(long)i * n + j] : 0.0;
-    }
+    team_copy_rows(tm, a.Q, ld, gQ, n, n, true);
+    team_copy_rows(tm, a.G, ld, gG, p, n, false);
     for (int i = tm.r; i < n; i += NT) a.q[i] = P->q[inst * n + i];
     for (int i = tm.r; i < p; i += NT) {
       a.h[i] = P->h[inst * p + i];
       a.zp[i] = 0.0;
     }
     pen = P->penalty[inst];
-    tm.sync();
-    for (int e = tm.r; e < n * n; e += NT) {
-      const int i = e / n, j = e - i * n;
-      if (j > i) {
-        const double v = 0.5 * (a.Q[i * ld + j] + a.Q[j * ld + i]);
-        a.Q[i * ld + j] = v;
-        a.Q[j * ld + i] = v;
-      }
-    }
     tm.sync();
   }
 

@@ -83,20 +83,9 @@ struct StdQP {
     const double* gG = P->G + R.oG;
     const double* gA = P->A + R.oA;
     const double* gh = P->h + R.oh;
-    for (int e = T.r; e < n * ld; e += NT) {
-      const int i = e / ld, j = e - i * ld;
-      a.Q[e] = (j < n) ? gQ[(long)i * n + j] : 0.0;
-    }
-    for (int e = T.r; e < p * ld; e += NT) {
-      const int i = e / ld, j = e - i * ld;
-      double v = (j < n) ? gG[(long)i * n + j] : 0.0;
-      if (remove_inf && isinf(gh[i])) v = 0.0;
-      a.G[e] = v;
-    }
-    for (int e = T.r; e < m * ld; e += NT) {
-      const int i = e / ld, j = e - i * ld;
-      a.A[e] = (j < n) ? gA[(long)i * n + j] : 0.0;
-    }
+    team_copy_rows(T, a.Q, ld, gQ, n, n, true);
+    team_copy_rows(T, a.G, ld, gG, p, n, false, [&](int i) { return remove_inf && isinf(__ldg(gh + i)); });
+    team_copy_rows(T, a.A, ld, gA, m, n, false);
     for (int i = T.r; i < n; i += NT) a.q[i] = P->q[R.oq + i];
     for (int i = T.r; i < m; i += NT) {
       a.b[i] = P->b[R.ob + i];
@@ -106,15 +95,6 @@ struct StdQP {
       const double hv = gh[i];
       a.h[i] = (remove_inf && isinf(hv)) ? 0.0 : hv;
       a.zp[i] = 0.0;
-    }
-    T.sync();
-    for (int e = T.r; e < n * n; e += NT) {
-      const int i = e / n, j = e - i * n;
-      if (j > i) {
-        const double v = 0.5 * (a.Q[i * ld + j] + a.Q[j * ld + i]);
-        a.Q[i * ld + j] = v;
-        a.Q[j * ld + i] = v;
-      }
     }
     T.sync();
   }

@@ -226,4 +226,43 @@ QPB_DEV double wv_dot(const WarpVec<kChunks>& a, const R* b, int n, int lane) {
   return acc;
 }
 
+// Copies a rows x n row-major source into dst with row stride ld (columns
+// n..ld-1 zeroed), kBatch elements per thread in flight: each batch's loads
+// are issued before its stores (source and destination are not known to be
+// distinct, so an element-at-a-time loop would wait for every load).  With
+// `sym` (rows == n) the copy is (S + S') / 2, each off-diagonal element
+// formed as 0.5 * (S[i][j] + S[j][i]); rows for which zero_row(i) holds are
+// written as zeros.
+struct NoZeroRows {
+  QPB_DEV bool operator()(int) const { return false; }
+};
+
+template <int NT, class ZeroRow = NoZeroRows>
+QPB_DEV void team_copy_rows(const Team<NT>& T, double* dst, int ld, const double* src, int rows, int n, bool sym,
+                            ZeroRow zero_row = ZeroRow()) {
+  constexpr int kBatch = 8;
+  const int total = rows * ld;
+  for (int e0 = T.r; e0 < total; e0 += NT * kBatch) {
+    double v[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int e = e0 + u * NT;
+      double x = 0.0;
+      if (e < total) {
+        const int i = e / ld, j = e - i * ld;
+        if (j < n && !zero_row(i)) {
+          x = __ldg(src + (long)i * n + j);
+          if (sym && i != j) x = 0.5 * (x + __ldg(src + (long)j * n + i));
+        }
+      }
+      v[u] = x;
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int e = e0 + u * NT;
+      if (e < total) dst[e] = v[u];
+    }
+  }
+}
+
 }  // namespace qpb

@@ -101,48 +101,127 @@ struct WarpQP {
     a.p = p;
   }
 
-  // sym(Q)[i][lane] through L1: (Q + Q')/2, or the coalesced Q[i][lane]
-  // alone when Q is exactly symmetric (checked once per instance).
-  QPB_DEV double qsym(int i) const {
-    if (!(i < n && lane < n)) return 0.0;
-    const double v = gQ[i * n + lane];
-    return q_symmetric ? v : 0.5 * (v + gQ[lane * n + i]);
+  // qv[i] = sym(Q)[i][lane]: (Q + Q')/2, or the coalesced Q[i][lane] alone
+  // when Q is exactly symmetric (checked once per instance).  All loads are
+  // issued before the first use: the column costs one L2 round trip.
+  QPB_DEV void load_q(double (&qv)[NP]) const {
+    const bool in = lane < n;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) qv[i] = (in && i < n) ? __ldg(gQ + i * n + lane) : 0.0;
+    if (!q_symmetric) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+        if (in && i < n) qv[i] = 0.5 * (qv[i] + __ldg(gQ + lane * n + i));
+    }
   }
   bool q_symmetric;
 
-  QPB_DEV void load(const InstRef& R, bool remove_inf) {
+  // L2 prefetch of instance i's operands (the next instance this warp
+  // solves), so that its load() finds them in L2.
+  QPB_DEV void prefetch(long i) const {
+    const InstRef R = inst_ref(*P, i);
+    auto pf = [&](const double* base, long count) {
+      for (long o = (long)lane * 16; o < count; o += 32 * 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + o));
+    };
+    pf(P->Q + R.oQ, (long)R.n * R.n);
+    pf(P->G + R.oG, (long)R.p * R.n);
+    pf(P->A + R.oA, (long)R.m * R.n);
+    pf(P->h + R.oh, R.p);
+  }
+
+  // 8-byte asynchronous copy global -> shared (dst must be shared memory).
+  static QPB_DEV void cp_async8(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+  }
+  static QPB_DEV void cp_async_wait_all() { asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory"); }
+
+  // Instance operands (and, with `iterate`, the starting iterate) into the
+  // arena.  A shared-memory arena is filled with asynchronous copies, every
+  // row in flight at once (one memory round trip per instance); a global
+  // arena (large p) with grouped loads.  Rows with h = inf are zeroed in G and
+  // h when remove_inf (qpax/pdip.py:166-178).
+  QPB_DEV void load(const InstRef& R, bool remove_inf, bool iterate) {
     gQ = P->Q + R.oQ;
     const double* gG = P->G + R.oG;
     const double* gA = P->A + R.oA;
     const double* gh = P->h + R.oh;
-    for (int r = 0; r < p; ++r) {
-      double v = (lane < n) ? gG[r * n + lane] : 0.0;
-      if (remove_inf && isinf(gh[r])) v = 0.0;
-      if (lane < NP) a.G()[r * NP + lane] = v;
-    }
+    if (P->arena_in_smem) {
+      for (int r = 0; r < p; ++r) {
+        if (lane < n)
+          cp_async8(a.G() + r * NP + lane, gG + r * n + lane);
+        else if (lane < NP)
+          a.G()[r * NP + lane] = 0.0;
+      }
 #pragma unroll
-    for (int i = 0; i < MP; ++i)
-      if (lane < NP) a.A()[i * NP + lane] = (i < m && lane < n) ? gA[i * n + lane] : 0.0;
-    for (int r = lane; r < p; r += 32) {
-      const double hv = gh[r];
-      a.h()[r] = (remove_inf && isinf(hv)) ? 0.0 : hv;
+      for (int i = 0; i < MP; ++i) {
+        if (i < m && lane < n)
+          cp_async8(a.A() + i * NP + lane, gA + i * n + lane);
+        else if (lane < NP)
+          a.A()[i * NP + lane] = 0.0;
+      }
+      for (int r = lane; r < p; r += 32) cp_async8(a.h() + r, gh + r);
+      if (iterate) {
+        for (int r = lane; r < p; r += 32) {
+          cp_async8(a.s() + r, P->in[1] + R.oh + r);
+          cp_async8(a.z() + r, P->in[2] + R.oh + r);
+        }
+      }
+      cp_async_wait_all();
+      // each lane copied G's column `lane` and h's rows lane, lane + 32, ...:
+      // the fix-up below touches only this lane's own copies
+      if (remove_inf) {
+        for (int r0 = 0; r0 < p; r0 += 32) {
+          const int r = r0 + lane;
+          const bool inf = r < p && isinf(a.h()[r]);
+          unsigned mask = __ballot_sync(kFull, inf);
+          while (mask) {
+            const int bit = __ffs(mask) - 1;
+            mask &= mask - 1;
+            if (lane < NP) a.G()[(r0 + bit) * NP + lane] = 0.0;
+          }
+          if (inf) a.h()[r] = 0.0;
+        }
+      }
+    } else {
+      // G rows in groups of 8: the group's loads are issued before its stores
+      for (int r0 = 0; r0 < p; r0 += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r0 + u;
+          v[u] = (r < p && lane < n) ? __ldg(gG + r * n + lane) : 0.0;
+          if (remove_inf && r < p && isinf(__ldg(gh + r))) v[u] = 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (r0 + u < p && lane < NP) a.G()[(r0 + u) * NP + lane] = v[u];
+      }
+#pragma unroll
+      for (int i = 0; i < MP; ++i)
+        if (lane < NP) a.A()[i * NP + lane] = (i < m && lane < n) ? gA[i * n + lane] : 0.0;
+      for (int r = lane; r < p; r += 32) {
+        const double hv = gh[r];
+        a.h()[r] = (remove_inf && isinf(hv)) ? 0.0 : hv;
+      }
+      if (iterate) {
+        for (int r = lane; r < p; r += 32) {
+          a.s()[r] = P->in[1][R.oh + r];
+          a.z()[r] = P->in[2][R.oh + r];
+        }
+      }
     }
     q = (lane < n) ? P->q[R.oq + lane] : 0.0;
     b = (lane < m) ? P->b[R.ob + lane] : 0.0;
-    int asym = 0;
-    if (lane < n)
-      for (int i = 0; i < n; ++i) asym |= (gQ[i * n + lane] != gQ[lane * n + i]);
-    q_symmetric = !__any_sync(kFull, asym);
-    __syncwarp();
-  }
-
-  QPB_DEV void load_iterate(const InstRef& R) {
-    x = (lane < n) ? P->in[0][R.oq + lane] : 0.0;
-    y = (lane < m) ? P->in[3][R.ob + lane] : 0.0;
-    for (int r = lane; r < p; r += 32) {
-      a.s()[r] = P->in[1][R.oh + r];
-      a.z()[r] = P->in[2][R.oh + r];
+    if (iterate) {
+      x = (lane < n) ? P->in[0][R.oq + lane] : 0.0;
+      y = (lane < m) ? P->in[3][R.ob + lane] : 0.0;
     }
+    int asym = 0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+      if (lane < n && i < n) asym |= (__ldg(gQ + i * n + lane) != __ldg(gQ + lane * n + i));
+    q_symmetric = !__any_sync(kFull, asym);
     __syncwarp();
   }
 
@@ -170,7 +249,7 @@ struct WarpQP {
                  : "d"(a0), "d"(b0));
   }
 
-  // hc[i] = (G' diag(w) G)[i][lane].  The lower-triangle 8x8 tiles are
+  // hc[i] += (G' diag(w) G)[i][lane].  The lower-triangle 8x8 tiles are
   // accumulated one tile row at a time on the FP64 tensor cores
   // (H_tile(ti, tj) = sum_k (w_k G[k][8ti..]) (x) G[k][8tj..]); each finished
   // tile row goes through the 8 x NP scratch (the Y region, rebuilt later in
@@ -208,21 +287,20 @@ struct WarpQP {
     const int tl = lane >> 3;  // this lane's tile column
     if (lane < NP && tl < TI) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) hc[8 * TI + r] = S[r * NP + lane];  // rows of tile row TI
+      for (int r = 0; r < 8; ++r) hc[8 * TI + r] += S[r * NP + lane];  // rows of tile row TI
     }
     if (lane < NP && tl == TI) {
       const int c = lane - 8 * TI;  // column within the diagonal tile
 #pragma unroll
-      for (int r = 0; r < 8; ++r) hc[8 * TI + r] = (r >= c) ? S[r * NP + lane] : S[c * NP + 8 * TI + r];
+      for (int r = 0; r < 8; ++r) hc[8 * TI + r] += (r >= c) ? S[r * NP + lane] : S[c * NP + 8 * TI + r];
 #pragma unroll
-      for (int i = 0; i < 8 * TI; ++i) hc[i] = S[c * NP + i];  // H[i][j] = H[j][i], i < 8TI
+      for (int i = 0; i < 8 * TI; ++i) hc[i] += S[c * NP + i];  // H[i][j] = H[j][i], i < 8TI
     }
     __syncwarp();
   }
 
+  // Adds G' diag(w) G to hc (each element of the column exactly once).
   QPB_DEV void form_h_tensor() {
-#pragma unroll
-    for (int i = 0; i < NP; ++i) hc[i] = 0.0;
     h_tile_row<0>();
     if constexpr (NP > 8) h_tile_row<1>();
     if constexpr (NP > 16) {
@@ -238,9 +316,16 @@ struct WarpQP {
     st_f64++;
     dinv = 0.0;
     fdinv = 0.0;
-    form_h_tensor();
+    // (starting from zeros rather than from Q keeps hc in registers)
 #pragma unroll
-    for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qsym(i) + hc[i];
+    for (int i = 0; i < NP; ++i) hc[i] = 0.0;
+    form_h_tensor();
+    {
+      double qv[NP];
+      load_q(qv);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qv[i] + hc[i];
+    }
     // LDL^T: step k broadcasts row k of the Schur complement (= column k)
     int bad = 0;
     double* cb = a.cb();
@@ -415,8 +500,12 @@ struct WarpQP {
   // qpax/pdip.py:93-100, pdip_relaxed.py:16-23.
   QPB_DEV double residuals(double kappa, double& v1, double& v4) {
     double qx = 0.0;
+    {
+      double qv[NP];
+      load_q(qv);
 #pragma unroll
-    for (int i = 0; i < NP; ++i) qx = fma(qsym(i), __shfl_sync(kFull, x, i), qx);
+      for (int i = 0; i < NP; ++i) qx = fma(qv[i], __shfl_sync(kFull, x, i), qx);
+    }
     double ay = 0.0;
 #pragma unroll
     for (int i = 0; i < MP; ++i) ay = fma(ycol_a(i), __shfl_sync(kFull, y, i), ay);
@@ -495,14 +584,13 @@ struct WarpQP {
     const long inst = R.id;
     const int op = P->op;
     const bool relaxed = (op == kOpRelax || op == kOpBwd);
-    load(R, op == kOpSolve);
+    const bool fresh = (op == kOpSolve || op == kOpInit);
+    load(R, op == kOpSolve, !fresh);
     int stage;
-    if (op == kOpSolve || op == kOpInit) {
+    if (fresh)
       stage = kInit;
-    } else {
-      load_iterate(R);
+    else
       stage = (op == kOpAdjoint) ? kAdjoint : kStep;
-    }
     if (op == kOpSolve && p == 0) stage = kInit;
     int it = 0, converged = 0, conv_now = 0;
     double v1 = 0.0, v4 = 0.0, dxr = 0.0, dyr = 0.0;
