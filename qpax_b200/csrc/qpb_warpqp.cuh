@@ -42,14 +42,16 @@ QPB_DEV double wmin(double v) {
 }
 
 // Shared-memory layout of one warp instance (doubles, in this order):
-//   G (p x NP) | A (MP x NP) | 9 p-vectors | xs, cb, dvi (NP each) |
-//   Y (MP x NP, Y[i][j] = (L^-1 A')[j][i]) | F (MP x MP, column-held factor)
+//   G (p x NP, columns swizzled: element (r, c) at r * NP + (c ^ gswz(r))) |
+//   A (MP x NP) | 9 p-vectors | xs, cb, dvi (NP each) |
+//   Y (MP x (NP + 1), Y[i][j] = (L^-1 A')[j][i]; the padded row stride keeps
+//   the F = Y D^-1 Y' reads in distinct banks) | F (MP x MP, column-held factor)
 // Addresses are recomputed from the base and p where used (no pointer table).
 struct WarpArena {
   static __host__ __device__ size_t doubles(int NP, int MP, int p) {
     // the Y region doubles as the 8 x NP tile-row scratch of the H formation
-    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + 3 * (size_t)NP + (size_t)(MP > 8 ? MP : 8) * NP +
-           (size_t)MP * MP;
+    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + 3 * (size_t)NP +
+           (size_t)(MP > 8 ? MP : 8) * (NP + 1) + (size_t)MP * MP;
   }
   static size_t bytes(int NP, int MP, int p) { return doubles(NP, MP, p) * sizeof(double) + 16; }
 };
@@ -76,12 +78,19 @@ struct WarpAddr {
   QPB_DEV double* cb() const { return xs() + NP; }
   QPB_DEV double* dvi() const { return xs() + 2 * NP; }
   QPB_DEV double* Y() const { return xs() + 3 * NP; }
-  QPB_DEV double* F() const { return Y() + (MP > 8 ? MP : 8) * NP; }
+  QPB_DEV double* F() const { return Y() + (MP > 8 ? MP : 8) * (NP + 1); }
 };
 
 template <int NP, int MP>
 struct WarpQP {
   static_assert(NP == 8 || NP == 16 || NP == 32, "NP");
+  static constexpr int kYld = NP + 1;  // row stride of Y
+  // Column swizzle of G's row r (period 4 in r): the four rows of one DMMA
+  // k-step fall in distinct shared-memory banks.
+  static QPB_DEV int gswz(int r) { return NP == 8 ? (r & 2) << 1 : (4 * r) & 12; }
+  // Column swizzle of row g of the H-formation scratch (fragment stores in
+  // distinct banks).
+  static QPB_DEV int sswz(int g) { return NP == 8 ? (g >> 1) & 1 : (g & 1) | ((g & 2) << 2); }
   const Params* P;
   WarpAddr<NP, MP> a;
   int n, m, p, lane;
@@ -149,9 +158,9 @@ struct WarpQP {
     if (P->arena_in_smem) {
       for (int r = 0; r < p; ++r) {
         if (lane < n)
-          cp_async8(a.G() + r * NP + lane, gG + r * n + lane);
+          cp_async8(a.G() + r * NP + (lane ^ gswz(r)), gG + r * n + lane);
         else if (lane < NP)
-          a.G()[r * NP + lane] = 0.0;
+          a.G()[r * NP + (lane ^ gswz(r))] = 0.0;
       }
 #pragma unroll
       for (int i = 0; i < MP; ++i) {
@@ -178,7 +187,7 @@ struct WarpQP {
           while (mask) {
             const int bit = __ffs(mask) - 1;
             mask &= mask - 1;
-            if (lane < NP) a.G()[(r0 + bit) * NP + lane] = 0.0;
+            if (lane < NP) a.G()[(r0 + bit) * NP + (lane ^ gswz(r0 + bit))] = 0.0;
           }
           if (inf) a.h()[r] = 0.0;
         }
@@ -195,7 +204,7 @@ struct WarpQP {
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u)
-          if (r0 + u < p && lane < NP) a.G()[(r0 + u) * NP + lane] = v[u];
+          if (r0 + u < p && lane < NP) a.G()[(r0 + u) * NP + (lane ^ gswz(r0 + u))] = v[u];
       }
 #pragma unroll
       for (int i = 0; i < MP; ++i)
@@ -265,21 +274,23 @@ struct WarpQP {
     double acc[TI + 1][2];
 #pragma unroll
     for (int tj = 0; tj <= TI; ++tj) acc[tj][0] = acc[tj][1] = 0.0;
+    const int sw = gswz(t);  // = gswz(4 kb + t)
     for (int kb = 0; kb < kblocks; ++kb) {
       const int k = 4 * kb + t;
       const bool in = k < p;
       const double* row = Gs + (in ? k : 0) * NP;
-      const double a0 = in ? wv[k] * row[8 * TI + g] : 0.0;  // (diag(w) G)'[8TI+g][k]
+      const double a0 = in ? wv[k] * row[(8 * TI + g) ^ sw] : 0.0;  // (diag(w) G)'[8TI+g][k]
 #pragma unroll
       for (int tj = 0; tj <= TI; ++tj) {
-        const double b0 = in ? row[8 * tj + g] : 0.0;  // G[k][8tj+g]
+        const double b0 = in ? row[(8 * tj + g) ^ sw] : 0.0;  // G[k][8tj+g]
         dmma884(acc[tj][0], acc[tj][1], a0, b0);
       }
     }
+    const int gs = sswz(g);
 #pragma unroll
     for (int tj = 0; tj <= TI; ++tj) {
-      S[g * NP + 8 * tj + 2 * t] = acc[tj][0];
-      S[g * NP + 8 * tj + 2 * t + 1] = acc[tj][1];
+      S[g * NP + ((8 * tj + 2 * t) ^ gs)] = acc[tj][0];
+      S[g * NP + ((8 * tj + 2 * t + 1) ^ gs)] = acc[tj][1];
     }
     __syncwarp();
     // Every element is taken from the lower triangle (row >= column) so that
@@ -287,14 +298,17 @@ struct WarpQP {
     const int tl = lane >> 3;  // this lane's tile column
     if (lane < NP && tl < TI) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) hc[8 * TI + r] += S[r * NP + lane];  // rows of tile row TI
+      for (int r = 0; r < 8; ++r) hc[8 * TI + r] += S[r * NP + (lane ^ sswz(r))];  // rows of tile row TI
     }
     if (lane < NP && tl == TI) {
       const int c = lane - 8 * TI;  // column within the diagonal tile
 #pragma unroll
-      for (int r = 0; r < 8; ++r) hc[8 * TI + r] += (r >= c) ? S[r * NP + lane] : S[c * NP + 8 * TI + r];
+      const int cs = sswz(c);
 #pragma unroll
-      for (int i = 0; i < 8 * TI; ++i) hc[i] += S[c * NP + i];  // H[i][j] = H[j][i], i < 8TI
+      for (int r = 0; r < 8; ++r)
+        hc[8 * TI + r] += (r >= c) ? S[r * NP + (lane ^ sswz(r))] : S[c * NP + ((8 * TI + r) ^ cs)];
+#pragma unroll
+      for (int i = 0; i < 8 * TI; ++i) hc[i] += S[c * NP + (i ^ cs)];  // H[i][j] = H[j][i], i < 8TI
     }
     __syncwarp();
   }
@@ -361,7 +375,7 @@ struct WarpQP {
     }
     if (lane < NP) {
 #pragma unroll
-      for (int i = 0; i < MP; ++i) a.Y()[i * NP + lane] = yc[i];
+      for (int i = 0; i < MP; ++i) a.Y()[i * kYld + lane] = yc[i];
     }
     __syncwarp();
     // F = Y D^-1 Y' (MP x MP, full storage, identity beyond m), one entry per lane
@@ -374,7 +388,7 @@ struct WarpQP {
       if (r < m && c < m) {
         double acc = 0.0;
 #pragma unroll 8
-        for (int j = 0; j < NP; ++j) acc = fma(Ys[r * NP + j] * dv[j], Ys[c * NP + j], acc);
+        for (int j = 0; j < NP; ++j) acc = fma(Ys[r * kYld + j] * dv[j], Ys[c * kYld + j], acc);
         v = acc;
       }
       Fm[e] = v;
@@ -395,7 +409,7 @@ struct WarpQP {
     if (bad) st_flags |= kFlagBreakdown64;
   }
 
-  QPB_DEV double ycol(int i) const { return lane < NP ? a.Y()[i * NP + lane] : 0.0; }
+  QPB_DEV double ycol(int i) const { return lane < NP ? a.Y()[i * kYld + lane] : 0.0; }
   QPB_DEV double fcol(int k) const { return lane < MP ? a.F()[k * MP + lane] : 0.0; }
 
   // --------------------------------------------------------- reduced solve
@@ -445,26 +459,38 @@ struct WarpQP {
   // Row dots G x with x in xs (rotated walk: conflict-free shared reads).
   QPB_DEV double grow_dot(int r, const double* xsv) const {
     const double* row = a.G() + r * NP;
+    const int sw = gswz(r);
     double g0 = 0.0, g1 = 0.0;
 #pragma unroll
     for (int t = 0; t < NP; t += 2) {
       const int c0 = (t + r) & (NP - 1), c1 = (t + 1 + r) & (NP - 1);
-      g0 = fma(row[c0], xsv[c0], g0);
-      g1 = fma(row[c1], xsv[c1], g1);
+      g0 = fma(row[c0 ^ sw], xsv[c0], g0);
+      g1 = fma(row[c1 ^ sw], xsv[c1], g1);
     }
     return g0 + g1;
   }
 
   // Column dots G' v (v in shared memory, length p), lane j.
   QPB_DEV double gcol_dot(const double* vv) const {
-    const double* Gc = a.G() + (lane < NP ? lane : 0);
-    double acc0 = 0.0, acc1 = 0.0;
+    const int c = lane < NP ? lane : 0;
+    const double* G = a.G();
+    // the column's position in row r repeats with period 4 (gswz)
+    const int c0 = c ^ gswz(0), c1 = c ^ gswz(1), c2 = c ^ gswz(2), c3 = c ^ gswz(3);
+    double acc0 = 0.0, acc1 = 0.0;  // even rows, odd rows
     int r = 0;
-    for (; r + 2 <= p; r += 2) {
-      acc0 = fma(Gc[r * NP], vv[r], acc0);
-      acc1 = fma(Gc[(r + 1) * NP], vv[r + 1], acc1);
+    for (; r + 4 <= p; r += 4) {
+      acc0 = fma(G[r * NP + c0], vv[r], acc0);
+      acc1 = fma(G[(r + 1) * NP + c1], vv[r + 1], acc1);
+      acc0 = fma(G[(r + 2) * NP + c2], vv[r + 2], acc0);
+      acc1 = fma(G[(r + 3) * NP + c3], vv[r + 3], acc1);
     }
-    if (r < p) acc0 = fma(Gc[r * NP], vv[r], acc0);
+    for (; r < p; ++r) {
+      const double g = G[r * NP + (c ^ gswz(r))];
+      if (r & 1)
+        acc1 = fma(g, vv[r], acc1);
+      else
+        acc0 = fma(g, vv[r], acc0);
+    }
     return acc0 + acc1;
   }
 
