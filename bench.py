@@ -619,8 +619,8 @@ def run_e2e(args, spec: Spec, data, dev, arm):
             qb.solve_qp_primal_vjp_host(*host, g_host, spec.tol, KAPPA, out=outs_host, chunks=args.e2e_chunks)
 
         path = (f"qpax_b200.solve_qp_primal_vjp_host -> qpb_solve_qp_primal_vjp_host (C ABI, host buffers): "
-                f"pinned host tensors, {args.e2e_chunks} chunks over 3 streams (copy in / solve + backward / copy "
-                "out overlap)")
+                f"pinned host tensors, {args.e2e_chunks} chunks: one copy-in stream, two compute streams taken in "
+                "turn, one copy-out stream (copies overlap the solves)")
     elif spec.kind == "elastic":
         host = [torch.tensor(a).pin_memory() for a in data] + [torch.full((B,), 1e3, dtype=torch.float64).pin_memory()]
         g_host = torch.full((B, spec.n), 0.1, dtype=torch.float64).pin_memory()

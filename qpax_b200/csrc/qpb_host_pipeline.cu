@@ -1,10 +1,18 @@
 // qpb_host_pipeline.cu -- forward + backward of solve_qp_primal on a batch held
 // in host memory: chunks of the batch flow through copy-in, the two solver
-// launches and copy-out on three internal streams, so that one chunk's copies
-// overlap another chunk's kernels (the host <-> device link is full duplex).
+// launches and copy-out on internal streams, so that one chunk's copies
+// overlap other chunks' kernels (the host <-> device link is full duplex).
+//
+// Streams by role: one copy-in stream (chunks arrive in order, each at the
+// link's full rate), two compute streams taken in turn (a chunk's solve can
+// start while the previous chunk's backward drains, filling the SMs its
+// tail leaves idle), one copy-out stream.  Chunks cycle through kSlots device
+// buffer sets; events order every reuse of a slot after the last reader of
+// its previous chunk.
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <vector>
 
 #include "../../include/qpb.h"
 #include "qpb_host.h"
@@ -12,16 +20,17 @@
 namespace qpb {
 namespace {
 
-constexpr int kSlots = 3;  // chunks in flight: copying in, computing, copying out
+constexpr int kSlots = 3;    // device buffer sets (chunks in flight)
+constexpr int kStreams = 4;  // copy-in, compute (two), copy-out
 
 // Internal streams of one device, created once (non-blocking: they never wait
 // on the legacy default stream).
 struct DeviceStreams {
-  cudaStream_t s[kSlots];
+  cudaStream_t s[kStreams];
   bool ok = false;
 };
 
-bool device_streams(cudaStream_t out[kSlots]) {
+bool device_streams(cudaStream_t out[kStreams]) {
   static DeviceStreams cache[64];
   static std::mutex mu;
   int dev = -1;
@@ -29,11 +38,11 @@ bool device_streams(cudaStream_t out[kSlots]) {
   std::lock_guard<std::mutex> lk(mu);
   DeviceStreams& d = cache[dev];
   if (!d.ok) {
-    for (int i = 0; i < kSlots; ++i)
+    for (int i = 0; i < kStreams; ++i)
       if (cudaStreamCreateWithFlags(&d.s[i], cudaStreamNonBlocking) != cudaSuccess) return false;
     d.ok = true;
   }
-  for (int i = 0; i < kSlots; ++i) out[i] = d.s[i];
+  for (int i = 0; i < kStreams; ++i) out[i] = d.s[i];
   return true;
 }
 
@@ -133,8 +142,10 @@ int qpb_solve_qp_primal_vjp_host(const qpb_dims* dims, const double* Q, const do
   if (need == 0) return QPB_ERR_UNSUPPORTED;
   if (!workspace || workspace_bytes < need || (reinterpret_cast<uintptr_t>(workspace) & 255))
     return QPB_ERR_WORKSPACE;
-  cudaStream_t ss[kSlots];
+  cudaStream_t ss[kStreams];
   if (!device_streams(ss)) return QPB_ERR_CUDA;
+  cudaStream_t s_in = ss[0], s_out = ss[3];
+  cudaStream_t s_comp[2] = {ss[1], ss[2]};
   const int S = slots_for(chunks);
   const long cap = chunk_cap(B, chunks);
   const size_t sb = slot_bytes(*dims, chunks, cfg);
@@ -143,69 +154,92 @@ int qpb_solve_qp_primal_vjp_host(const qpb_dims* dims, const double* Q, const do
     const qpb_dims dc{(int32_t)cap, dims->n, dims->m, dims->p};
     slots[k].carve(reinterpret_cast<unsigned char*>(workspace) + k * sb, cap, n, m, p, solver_ws(dc, cfg));
   }
-  // fork: the slot streams start after the work already queued on `stream`
-  cudaStream_t s0 = reinterpret_cast<cudaStream_t>(stream);
-  cudaEvent_t fork, join[kSlots];
-  if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess) return QPB_ERR_CUDA;
-  int made = 0;
+  // per chunk: inputs on the device (in), x computed (x), backward done
+  // (done), outputs copied (out); plus the fork and one join per stream
+  enum { kIn, kX, kDone, kOut, kKinds };
+  std::vector<cudaEvent_t> ev;
+  const size_t n_ev = (size_t)chunks * kKinds + 1 + kStreams;
+  ev.reserve(n_ev);
   st = QPB_OK;
-  for (; made < S; ++made)
-    if (cudaEventCreateWithFlags(&join[made], cudaEventDisableTiming) != cudaSuccess) {
+  for (size_t i = 0; i < n_ev; ++i) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
       st = QPB_ERR_CUDA;
       break;
     }
+    ev.push_back(e);
+  }
+  auto E = [&](int c, int kind) { return ev[(size_t)c * kKinds + kind]; };
+  cudaEvent_t fork = st == QPB_OK ? ev[(size_t)chunks * kKinds] : nullptr;
+  // fork: the internal streams start after the work already queued on `stream`
+  cudaStream_t s0 = reinterpret_cast<cudaStream_t>(stream);
   if (st == QPB_OK && cudaEventRecord(fork, s0) != cudaSuccess) st = QPB_ERR_CUDA;
-  for (int k = 0; st == QPB_OK && k < S; ++k)
+  for (int k = 0; st == QPB_OK && k < kStreams; ++k)
     if (cudaStreamWaitEvent(ss[k], fork, 0) != cudaSuccess) st = QPB_ERR_CUDA;
   for (int c = 0; st == QPB_OK && c < chunks; ++c) {
     const long lo = B * c / chunks, hi = B * (c + 1) / chunks, cnt = hi - lo;
-    if (cnt <= 0) continue;
     const Slot& sl = slots[c % S];
-    cudaStream_t s = ss[c % S];
+    cudaStream_t sc = s_comp[c & 1];
     const qpb_dims dc{(int32_t)cnt, dims->n, dims->m, dims->p};
-    // copy in (instances lo .. hi-1 are contiguous in every array)
     cudaError_t e = cudaSuccess;
-    e = e ? e : copy_in(sl.Q, Q + lo * n * n, cnt * n * n * 8, s);
-    e = e ? e : copy_in(sl.q, q + lo * n, cnt * n * 8, s);
-    e = e ? e : copy_in(sl.A, A + lo * m * n, cnt * m * n * 8, s);
-    e = e ? e : copy_in(sl.b, b + lo * m, cnt * m * 8, s);
-    e = e ? e : copy_in(sl.G, G + lo * p * n, cnt * p * n * 8, s);
-    e = e ? e : copy_in(sl.h, h + lo * p, cnt * p * 8, s);
-    e = e ? e : copy_in(sl.dl, dl_dx + lo * n, cnt * n * 8, s);
+    // copy in (instances lo .. hi-1 are contiguous in every array), once the
+    // slot's previous chunk no longer reads its inputs
+    if (c >= S) e = cudaStreamWaitEvent(s_in, E(c - S, kDone), 0);
+    e = e ? e : copy_in(sl.Q, Q + lo * n * n, cnt * n * n * 8, s_in);
+    e = e ? e : copy_in(sl.q, q + lo * n, cnt * n * 8, s_in);
+    e = e ? e : copy_in(sl.A, A + lo * m * n, cnt * m * n * 8, s_in);
+    e = e ? e : copy_in(sl.b, b + lo * m, cnt * m * 8, s_in);
+    e = e ? e : copy_in(sl.G, G + lo * p * n, cnt * p * n * 8, s_in);
+    e = e ? e : copy_in(sl.h, h + lo * p, cnt * p * 8, s_in);
+    e = e ? e : copy_in(sl.dl, dl_dx + lo * n, cnt * n * 8, s_in);
+    e = e ? e : cudaEventRecord(E(c, kIn), s_in);
+    // compute, once the inputs are in and the slot's previous outputs are out
+    e = e ? e : cudaStreamWaitEvent(sc, E(c, kIn), 0);
+    if (c >= S) e = e ? e : cudaStreamWaitEvent(sc, E(c - S, kOut), 0);
     if (e != cudaSuccess) {
       st = QPB_ERR_CUDA;
       break;
     }
-    st = qpb_solve_qp(&dc, sl.Q, sl.q, sl.A, sl.b, sl.G, sl.h, solver_tol, sl.x, sl.s, sl.z, sl.y, sl.conv,
-                      sl.iters, cfg, sl.ws, sl.ws_bytes, reinterpret_cast<qpb_stream_t>(s));
-    if (st) break;
-    if (converged) e = e ? e : copy_out(converged + lo, sl.conv, cnt * 4, s);
-    if (iters) e = e ? e : copy_out(iters + lo, sl.iters, cnt * 4, s);
-    e = e ? e : copy_out(x + lo * n, sl.x, cnt * n * 8, s);
-    if (e != cudaSuccess) {
-      st = QPB_ERR_CUDA;
-      break;
+    if (cnt > 0) {
+      st = qpb_solve_qp(&dc, sl.Q, sl.q, sl.A, sl.b, sl.G, sl.h, solver_tol, sl.x, sl.s, sl.z, sl.y, sl.conv,
+                        sl.iters, cfg, sl.ws, sl.ws_bytes, reinterpret_cast<qpb_stream_t>(sc));
+      if (st) break;
     }
-    st = qpb_solve_qp_primal_bwd(&dc, sl.Q, sl.q, sl.A, sl.b, sl.G, sl.h, sl.x, sl.s, sl.z, sl.y, sl.dl, solver_tol,
-                                 target_kappa, sl.dQ, sl.dq, sl.dA, sl.db, sl.dG, sl.dh, nullptr, nullptr, nullptr,
-                                 nullptr, nullptr, nullptr, cfg, sl.ws, sl.ws_bytes, reinterpret_cast<qpb_stream_t>(s));
-    if (st) break;
-    e = e ? e : copy_out(dQ + lo * n * n, sl.dQ, cnt * n * n * 8, s);
-    e = e ? e : copy_out(dq + lo * n, sl.dq, cnt * n * 8, s);
-    e = e ? e : copy_out(dA + lo * m * n, sl.dA, cnt * m * n * 8, s);
-    e = e ? e : copy_out(db + lo * m, sl.db, cnt * m * 8, s);
-    e = e ? e : copy_out(dG + lo * p * n, sl.dG, cnt * p * n * 8, s);
-    e = e ? e : copy_out(dh + lo * p, sl.dh, cnt * p * 8, s);
+    e = cudaEventRecord(E(c, kX), sc);
+    if (cnt > 0 && e == cudaSuccess) {
+      st = qpb_solve_qp_primal_bwd(&dc, sl.Q, sl.q, sl.A, sl.b, sl.G, sl.h, sl.x, sl.s, sl.z, sl.y, sl.dl,
+                                   solver_tol, target_kappa, sl.dQ, sl.dq, sl.dA, sl.db, sl.dG, sl.dh, nullptr,
+                                   nullptr, nullptr, nullptr, nullptr, nullptr, cfg, sl.ws, sl.ws_bytes,
+                                   reinterpret_cast<qpb_stream_t>(sc));
+      if (st) break;
+    }
+    e = e ? e : cudaEventRecord(E(c, kDone), sc);
+    // copy out: x as soon as the forward is done, the gradients after the backward
+    e = e ? e : cudaStreamWaitEvent(s_out, E(c, kX), 0);
+    if (converged) e = e ? e : copy_out(converged + lo, sl.conv, cnt * 4, s_out);
+    if (iters) e = e ? e : copy_out(iters + lo, sl.iters, cnt * 4, s_out);
+    e = e ? e : copy_out(x + lo * n, sl.x, cnt * n * 8, s_out);
+    e = e ? e : cudaStreamWaitEvent(s_out, E(c, kDone), 0);
+    e = e ? e : copy_out(dQ + lo * n * n, sl.dQ, cnt * n * n * 8, s_out);
+    e = e ? e : copy_out(dq + lo * n, sl.dq, cnt * n * 8, s_out);
+    e = e ? e : copy_out(dA + lo * m * n, sl.dA, cnt * m * n * 8, s_out);
+    e = e ? e : copy_out(db + lo * m, sl.db, cnt * m * 8, s_out);
+    e = e ? e : copy_out(dG + lo * p * n, sl.dG, cnt * p * n * 8, s_out);
+    e = e ? e : copy_out(dh + lo * p, sl.dh, cnt * p * 8, s_out);
+    e = e ? e : cudaEventRecord(E(c, kOut), s_out);
     if (e != cudaSuccess) st = QPB_ERR_CUDA;
   }
-  // join: `stream` continues after every slot's last copy-out (also on error,
-  // so that nothing queued here outlives the caller's view of the stream)
-  for (int k = 0; k < made; ++k) {
-    if (cudaEventRecord(join[k], ss[k]) != cudaSuccess || cudaStreamWaitEvent(s0, join[k], 0) != cudaSuccess)
-      st = st ? st : QPB_ERR_CUDA;
-    cudaEventDestroy(join[k]);
+  // join: `stream` continues after everything queued on the internal streams
+  // (also on error, so that nothing queued here outlives the caller's view of
+  // the stream)
+  if (ev.size() == n_ev) {
+    for (int k = 0; k < kStreams; ++k) {
+      cudaEvent_t j = ev[(size_t)chunks * kKinds + 1 + k];
+      if (cudaEventRecord(j, ss[k]) != cudaSuccess || cudaStreamWaitEvent(s0, j, 0) != cudaSuccess)
+        st = st ? st : QPB_ERR_CUDA;
+    }
   }
-  cudaEventDestroy(fork);
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
   return st;
 }
 
