@@ -653,7 +653,7 @@ def run_e2e(args, spec: Spec, data, dev, arm):
             pipe.run(*host, g_host, spec.tol, KAPPA, out=outs_host)
 
         path = (f"qpax_b200.packed.PackedHostPipeline (C ABI plans): packed pinned host tensors, {args.e2e_chunks} "
-                "instance groups over 3 streams (copy in / solve + backward / copy out overlap)")
+                "instance groups: one copy-in stream, two compute streams taken in turn, one copy-out stream")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -687,7 +687,7 @@ def main():
     if args.e2e_chunks <= 0:
         # copies of the large workloads overlap best in 4-8 slices; small
         # ones want few slices (each slice's launch must still fill the GPU)
-        args.e2e_chunks = {"dense": 4, "nnls": 2, "small": 2, "uneven": 8, "elastic": 1}[spec.key]
+        args.e2e_chunks = {"dense": 4, "nnls": 4, "small": 2, "uneven": 8, "elastic": 1}[spec.key]
     if args.batch > 0 and args.batch != spec.batch:
         spec = Spec(spec.key, spec.kind, args.batch, spec.n, spec.m, spec.p, spec.tol,
                     spec.workload.replace(f"{spec.batch}", f"{args.batch}", 1))

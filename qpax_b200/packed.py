@@ -149,9 +149,11 @@ class PackedHostPipeline:
     memory, with copies overlapped with the kernels.
 
     The instances are cut into `chunks` contiguous groups (contiguous in every
-    packed array), each with its own plan and device buffers; on three
-    streams each group is copied in, solved forward and backward, and its x and
-    six gradients copied back while the other groups compute.
+    packed array), each with its own plan and device buffers.  Streams by
+    role: the groups are copied in, in order, on one stream (each at the
+    link's full rate), solved forward and backward on compute streams taken
+    in turn (one group's solve overlaps the previous group's tail), and their
+    x and six gradients copied back on a last stream.
 
         pipe = PackedHostPipeline(shapes, chunks=4)
         x, grads = pipe.run(Q, q, A, b, G, h, dl_dx, solver_tol, target_kappa, out=None)
@@ -160,7 +162,7 @@ class PackedHostPipeline:
     overlap); `out` may hold packed CPU tensors (x, dQ, dq, dA, db, dG, dh).
     """
 
-    def __init__(self, shapes, chunks: int = 4, precision: str = "auto", streams: int = 3):
+    def __init__(self, shapes, chunks: int = 4, precision: str = "auto", streams: int = 4):
         sh = np.ascontiguousarray(np.asarray(shapes, dtype=np.int32).reshape(-1, 3))
         B = sh.shape[0]
         chunks = max(1, min(int(chunks), B))
@@ -171,7 +173,8 @@ class PackedHostPipeline:
         self.offs = [np.concatenate([[0], np.cumsum(v)]) for v in self.lengths]
         self.plans = [PackedPlan(sh[lo:hi], precision) for lo, hi in zip(self.bounds[:-1], self.bounds[1:])]
         self.dev = _lib.device()
-        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(max(1, streams))]
+        # copy-in, compute (streams - 2 of them, at least one), copy-out
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(max(3, streams))]
         # field of each input / output: Q q A b G h dl -> 0 1 2 3 4 5 1; x dQ dq dA db dG dh -> 1 0 1 2 3 4 5
         self.in_fields = [0, 1, 2, 3, 4, 5, 1]
         self.out_fields = [1, 0, 1, 2, 3, 4, 5]
@@ -190,21 +193,30 @@ class PackedHostPipeline:
         main = torch.cuda.current_stream(self.dev)
         for s in self.streams:
             s.wait_stream(main)
+        s_in, s_out, comp = self.streams[0], self.streams[-1], self.streams[1:-1]
         for c, plan in enumerate(self.plans):
-            s = self.streams[c % len(self.streams)]
-            with torch.cuda.stream(s):
-                d = self.dev_in[c]
+            d = self.dev_in[c]
+            with torch.cuda.stream(s_in):
                 for dst, src, f in zip(d, host_in, self.in_fields):
                     lo, hi = self._span(f, c)
                     dst.copy_(src[lo:hi], non_blocking=True)
+            arrived = torch.cuda.Event()
+            arrived.record(s_in)
+            sc = comp[c % len(comp)]
+            sc.wait_event(arrived)
+            with torch.cuda.stream(sc):
                 res = plan.solve(*d[:6], solver_tol)
                 grads = plan.primal_bwd(*d[:6], *res[:4], d[6], solver_tol, target_kappa)
+            solved = torch.cuda.Event()
+            solved.record(sc)
+            s_out.wait_event(solved)
+            with torch.cuda.stream(s_out):
                 for dst, src, f in zip(out, (res[0],) + tuple(grads), self.out_fields):
                     lo, hi = self._span(f, c)
                     dst[lo:hi].copy_(src, non_blocking=True)
-                    src.record_stream(s)
+                    src.record_stream(s_out)
                 for t in res:
-                    t.record_stream(s)
+                    t.record_stream(s_out)
         for s in self.streams:
             main.wait_stream(s)
         torch.cuda.synchronize(self.dev)
