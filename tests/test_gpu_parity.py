@@ -161,6 +161,35 @@ def test_blocked_factorisation_shapes(prec, shape):
         assert_close(np_(g)[ok], go[ok], G_TOL, name)
 
 
+def test_warp_kernel_global_arena():
+    """n <= 32 with p = 200: the one-warp-per-instance kernel's arena (71 KB)
+    no longer fits four to a CTA in shared memory and lives in global memory
+    (grouped loads instead of asynchronous staging).  Forward with h = inf
+    rows (qpax/pdip.py:166-178, :243-246) and the VJP, vs the oracle."""
+    import qpax_b200 as qb
+
+    Q, q, A, b, G, h = wl.dense(8, 24, 4, 200, 901)
+    hi = h.copy()
+    hi[:, 5] = np.inf
+    hi[2, 17] = np.inf
+    x, s, z, y, conv, iters = (np_(t) for t in qb.solve_qp(Q, q, A, b, G, hi, 1e-6))
+    ref = oracle.solve_qp(Q, q, A, b, G, hi, solver_tol=1e-6)
+    np.testing.assert_array_equal(conv, ref[4])
+    np.testing.assert_array_equal(iters, ref[5])
+    fin = np.isfinite(hi)
+    np.testing.assert_array_equal(np.isinf(s), ~fin)
+    np.testing.assert_array_equal(z[~fin], 0.0)
+    assert_close(x, ref[0], X_TOL, "x")
+    assert_close(y, ref[3], X_TOL, "y")
+    assert_close(np.where(fin, s, 0.0), np.where(fin, ref[1], 0.0), X_TOL, "s")
+    assert_close(z, ref[2], X_TOL, "z")
+    (xv, grads, convv, _), (x_o, grads_o, conv_o, _) = _vjp_pair(Q, q, A, b, G, h, 1e-6, 1e-3, "auto")
+    np.testing.assert_array_equal(np_(convv), conv_o)
+    assert_close(xv, x_o, X_TOL, "x (vjp)")
+    for g, go, name in zip(grads, grads_o, ["dQ", "dq", "dA", "db", "dG", "dh"]):
+        assert_close(g, go, G_TOL, name)
+
+
 @pytest.mark.parametrize("prec", PRECS)
 def test_elastic_blocked_global_arena(prec):
     """Elastic QPs large enough for the blocked factorisation from a global
