@@ -128,14 +128,18 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
   const int np = warp_np(d);
   if (!elastic && !mixed && np && (cfg.team_threads == 0 || cfg.team_threads == 32)) {
-    // one warp per instance, FP64, several instances per CTA
-    KernelFn fn = kernel_warp_f64(np);
+    // one warp per instance (n_pad = 16, 32) or four instances per warp in
+    // lockstep (n_pad = 8), FP64, four warps per CTA; `teams` counts
+    // instances per CTA
+    KernelFn gfn = kernel_group_f64(np);
+    const int per_warp = gfn ? 32 / np : 1;
+    KernelFn fn = gfn ? gfn : kernel_warp_f64(np);
     if (!fn) return QPB_ERR_UNSUPPORTED;
     size_t arena = (WarpArena::bytes(np, np / 4, d.p) + 255) & ~size_t(255);
     pl->fn = (const void*)fn;
     pl->NT = 32;
     pl->arena_bytes = arena;
-    pl->teams = kWarpKernelThreads / 32;
+    pl->teams = (kWarpKernelThreads / 32) * per_warp;
     pl->threads = kWarpKernelThreads;
     if (arena * pl->teams <= smem_budget) {
       pl->in_smem = 1;

@@ -125,19 +125,6 @@ struct WarpQP {
   }
   bool q_symmetric;
 
-  // L2 prefetch of instance i's operands (the next instance this warp
-  // solves), so that its load() finds them in L2.
-  QPB_DEV void prefetch(long i) const {
-    const InstRef R = inst_ref(*P, i);
-    auto pf = [&](const double* base, long count) {
-      for (long o = (long)lane * 16; o < count; o += 32 * 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + o));
-    };
-    pf(P->Q + R.oQ, (long)R.n * R.n);
-    pf(P->G + R.oG, (long)R.p * R.n);
-    pf(P->A + R.oA, (long)R.m * R.n);
-    pf(P->h + R.oh, R.p);
-  }
-
   // 8-byte asynchronous copy global -> shared (dst must be shared memory).
   static QPB_DEV void cp_async8(double* dst, const double* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
@@ -302,7 +289,6 @@ struct WarpQP {
     }
     if (lane < NP && tl == TI) {
       const int c = lane - 8 * TI;  // column within the diagonal tile
-#pragma unroll
       const int cs = sswz(c);
 #pragma unroll
       for (int r = 0; r < 8; ++r)
