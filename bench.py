@@ -536,9 +536,11 @@ def run_ours(args, spec: Spec, world, rank, local):
         "traffic": (traffic or {}).get(dom_key),
         "traffic_source": (traffic or {}).get("source"),
     }
-    prec_desc = {"uniform": "auto (FP64; one warp per QP for n <= 32, one CTA per QP above)",
+    prec_desc = {"uniform": "auto (FP64; four QPs per warp for n <= 8, one warp per QP for n <= 32, one CTA per QP "
+                            "above)",
                  "elastic": "auto (FP64, one CTA per QP)",
-                 "uneven": "auto (FP64; per size bin: one warp per QP for n <= 32, one CTA per QP above)"}[spec.kind]
+                 "uneven": "auto (FP64; per size bin: four QPs per warp for n <= 8, one warp per QP for n <= 32, "
+                           "one CTA per QP above)"}[spec.kind]
     line = {
         "metric": metric_for(spec), "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": main_r["total_ms"] / args.steps, "higher_is_better": True,

@@ -41,8 +41,8 @@ typedef enum {
 } qpb_status;
 
 /* AUTO picks, per problem size, the fastest path that meets FP64 accuracy:
- * today the FP64 kernels (one warp per instance for n <= 32, m <= n_pad/4;
- * one CTA per instance above).  MIXED forces FP32 factorisation with FP64
+ * today the FP64 kernels (four instances per warp for n <= 8, m <= 2; one
+ * warp per instance for n <= 32, m <= n_pad/4; one CTA per instance above).  MIXED forces FP32 factorisation with FP64
  * refinement; FP64 forces FP64 factorisation. */
 typedef enum { QPB_PRECISION_AUTO = 0, QPB_PRECISION_MIXED = 1, QPB_PRECISION_FP64 = 2 } qpb_precision;
 
