@@ -77,6 +77,53 @@ def test_uneven_backward_matches_oracle():
         _close(unpack(grads[k], L[k]), grads_o[k], ok, 1e-5, name)
 
 
+def _small_batch(count, seed):
+    """Instances with n <= 8 (the four-per-warp lockstep kernel): n, m, p all
+    vary, so the groups of one warp hold different shapes (p >= 1: packed
+    batches carry inequalities)."""
+    rng = np.random.default_rng(seed)
+    data = [[], [], [], [], [], []]
+    for i in range(count):
+        n = int(rng.integers(1, 9))
+        m = int(rng.integers(0, min(2, n - 1) + 1)) if n > 1 else 0
+        p = int(rng.integers(1, 21))
+        inst = wl.dense(1, n, m, p, rng)
+        for k in range(6):
+            data[k].append(inst[k][0])
+    return data
+
+
+def test_lockstep_groups_with_mixed_shapes():
+    """37 instances with n <= 8 (the last warp partly empty), shapes varying
+    within every warp: forward, then forward + backward, vs the oracle."""
+    from qpax_b200.packed import PackedPlan, pack, unpack, solve_qp_uneven
+
+    data = _small_batch(37, 21)
+    xs, ss, zs, ys, conv, iters = solve_qp_uneven(*data, solver_tol=1e-6)
+    ref = oracle.solve_qp(*data, solver_tol=1e-6)
+    ok = np.asarray(ref[4]) == 1
+    assert ok.mean() >= 0.9
+    np.testing.assert_array_equal(conv.cpu().numpy()[ok], 1)
+    np.testing.assert_array_equal(iters.cpu().numpy()[ok], np.asarray(ref[5])[ok])
+    for g, r, name in zip((xs, ss, zs, ys), ref[:4], "xszy"):
+        _close(g, r, ok, 1e-6, name)
+
+    data = _small_batch(37, 22)
+    shapes = [(len(q), len(b), len(h)) for q, b, h in zip(data[1], data[3], data[5])]
+    plan = PackedPlan(shapes)
+    ins = [pack(v) for v in data]
+    x, s, z, y, conv, iters = plan.solve(*ins, 1e-6)
+    x_ref = oracle.solve_qp(*data, solver_tol=1e-6)
+    dl = [wl.loss_grad(v) for v in x_ref[0]]
+    grads = plan.primal_bwd(*ins, x, s, z, y, pack(dl), 1e-6, 1e-3)
+    _, grads_o, conv_o, _ = oracle.solve_qp_primal_vjp(*data, dl, solver_tol=1e-6, target_kappa=1e-3)
+    ok = np.asarray(conv_o) == 1
+    assert ok.mean() >= 0.9
+    L = plan.lengths
+    for k, name in enumerate(["dQ", "dq", "dA", "db", "dG", "dh"]):
+        _close(unpack(grads[k], L[k]), grads_o[k], ok, 1e-5, name)
+
+
 def test_cuda_graph_replay_matches_eager():
     from qpax_b200.packed import PackedPlan, pack
 
