@@ -566,8 +566,10 @@ def run_ours(args, spec: Spec, world, rank, local):
         line["converged_flags_identical"] = bool(all((r["conv"] == main_r["conv"]).all() for r in results.values()))
         line["iteration_counts_identical"] = bool(all((r["iters"] == main_r["iters"]).all()
                                                       for r in results.values()))
-    if rank == 0 and not args.no_e2e:
-        line["e2e"] = run_e2e(args, spec, data, dev, arm_main)
+    if not args.no_e2e:  # every rank takes part (barriers, max over ranks)
+        e2e = run_e2e(args, spec, data, dev, arm_main, world)
+        if rank == 0:
+            line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(spec, data)
     if rank == 0:
@@ -599,7 +601,7 @@ def simt_peaks():
     return out
 
 
-def run_e2e(args, spec: Spec, data, dev, arm):
+def run_e2e(args, spec: Spec, data, dev, arm, world=1):
     """Same metric through the public API from pinned host buffers: H2D of the
     inputs and the incoming gradient, forward + backward, D2H of x and the
     gradients, all inside the timed region."""
@@ -660,14 +662,18 @@ def run_e2e(args, spec: Spec, data, dev, arm):
         step()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    barrier(world)
+    torch.cuda.synchronize()
     e0.record()
     for _ in range(args.steps):
         step()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    return {"value": B * args.steps / (ms * 1e-3), "unit": "QPs/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.steps, "path": path}
+    barrier(world)
+    ms = barrier_max(e0.elapsed_time(e1), world)  # every rank copies and solves its own batch
+    return {"value": world * B * args.steps / (ms * 1e-3), "unit": "QPs/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "bytes_counted": "per rank (each rank copies its own batch)",
+            "ms_per_step": ms / args.steps, "path": path}
 
 
 def main():
