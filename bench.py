@@ -284,7 +284,7 @@ def run_reference(args, spec: Spec, world, rank):
         "impl": "reference", "metric": metric_for(spec), "value": val, "unit": "QPs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_for(spec, 1, extra={"workload": spec.workload + " (all host threads)"}),
+        "config": config_for(spec, 1),
         "cpu_baseline": {"value": val, "unit": "QPs/s", "cores": cores, "kind": "port",
                          "sample": f"the first {per_step} QPs of the batch per step, {args.steps} steps"},
         "e2e": {"value": val, "unit": "QPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -349,6 +349,7 @@ class UniformArm:
         self.conv, self.iters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
         self.rconv, self.riters = bt.new(B, dtype=torch.int32), bt.new(B, dtype=torch.int32)
         self.gx = torch.empty(B, n, dtype=torch.float64, device=dev)
+        self.grads = None
         self.launches = 2
 
     def fwd(self):
@@ -363,11 +364,19 @@ class UniformArm:
         from qpax_b200.diff_qp import diff_qp_from_forward
 
         torch.mul(self.x - 1.0, 2.0, out=self.gx)
-        diff_qp_from_forward(self.bt, self.x, self.s, self.z, self.y, self.gx, self.spec.tol, KAPPA, self.opts,
-                             relaxed=[None, None, None, None, self.rconv, self.riters])
+        self.grads = diff_qp_from_forward(self.bt, self.x, self.s, self.z, self.y, self.gx, self.spec.tol, KAPPA,
+                                          self.opts, relaxed=[None, None, None, None, self.rconv, self.riters])
 
     def counts(self):
         return self.conv.cpu().numpy(), self.iters.cpu().numpy(), self.riters.cpu().numpy()
+
+    def parity(self, data, limit=None):
+        """Figures of the last step's outputs against the oracle, given the same dl/dx."""
+        from oracle import parity
+
+        dl = self.gx.cpu().numpy()
+        return parity.standard(data, self.spec.tol, KAPPA, dl, self.x.cpu().numpy(), self.conv.cpu().numpy(),
+                               self.iters.cpu().numpy(), [g.cpu().numpy() for g in self.grads])[0]
 
     def kernel_name(self, which):
         return "qpb_solve_qp (forward)" if which == "forward" else "qpb_solve_qp_primal_bwd (backward)"
@@ -387,6 +396,7 @@ class ElasticArm:
         self.bt = ElasticBatch(*self.dev_in, self.pen)
         self.gx = torch.empty(spec.batch, spec.n, dtype=torch.float64, device=dev)
         self.out = None
+        self.grads = None
         self.launches = 2
 
     def fwd(self):
@@ -400,7 +410,8 @@ class ElasticArm:
         from qpax_b200.elastic_qp import _elastic_bwd
 
         torch.mul(self.out[0] - 1.0, 2.0, out=self.gx)
-        _elastic_bwd(self.bt, [t.contiguous() for t in self.out[:6]], self.gx, self.spec.tol, KAPPA, self.opts)
+        self.grads = _elastic_bwd(self.bt, [t.contiguous() for t in self.out[:6]], self.gx, self.spec.tol, KAPPA,
+                                  self.opts)
 
     def counts(self):
         import qpax_b200 as qb
@@ -409,13 +420,21 @@ class ElasticArm:
         rel = qb.relax_qp_elastic(*self.dev_in, self.pen, *self.out[:6], self.spec.tol, KAPPA, **self.opts)
         return conv, iters, rel[7].cpu().numpy()
 
+    def parity(self, data, limit=None):
+        from oracle import parity
+
+        return parity.elastic(tuple(data), 1e3, self.spec.tol, KAPPA, self.gx.cpu().numpy(),
+                              [t.cpu().numpy() for t in self.out], [g.cpu().numpy() for g in self.grads])[0]
+
     def kernel_name(self, which):
         return ("qpb_solve_qp_elastic (forward)" if which == "forward"
                 else "qpb_solve_qp_elastic_primal_bwd (backward)")
 
 
 class UnevenArm:
-    """Packed plan: every size bin of the batch launched concurrently."""
+    """Packed plan: every size bin of the batch launched concurrently.  The
+    forward call and the backward call (with the loss gradient between them)
+    are each captured once in a CUDA graph and replayed every step."""
 
     def __init__(self, spec: Spec, data, dev, opts):
         import torch
@@ -431,26 +450,65 @@ class UnevenArm:
         self.rconv = torch.empty(B, dtype=torch.int32, device=dev)
         self.riters = torch.empty(B, dtype=torch.int32, device=dev)
         self.gx = torch.empty(self.plan.totals[1], dtype=torch.float64, device=dev)
-        self.out = None
         self.launches = 2 * self.plan.num_bins
+        # eager warm-up on a side stream, then capture forward and backward
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            self._fwd_eager()
+            self._bwd_eager()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        self.g_fwd, self.g_bwd = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g_fwd):
+            self._fwd_eager()
+        with torch.cuda.graph(self.g_bwd, pool=self.g_fwd.pool()):
+            self._bwd_eager()
+        torch.cuda.synchronize(dev)
 
-    def fwd(self):
+    def _fwd_eager(self):
         self.out = self.plan.solve(*self.ins, self.spec.tol)
 
-    def bwd(self):
+    def _bwd_eager(self):
         import torch
 
         torch.mul(self.out[0] - 1.0, 2.0, out=self.gx)
-        self.plan.primal_bwd(*self.ins, *self.out[:4], self.gx, self.spec.tol, KAPPA,
-                             relax_out=(self.rconv, self.riters))
+        self.grads = self.plan.primal_bwd(*self.ins, *self.out[:4], self.gx, self.spec.tol, KAPPA,
+                                          relax_out=(self.rconv, self.riters))
+
+    def fwd(self):
+        self.g_fwd.replay()
+
+    def bwd(self):
+        self.g_bwd.replay()
+
+    def release(self):
+        self.g_fwd, self.g_bwd = None, None
 
     def counts(self):
         return self.out[4].cpu().numpy(), self.out[5].cpu().numpy(), self.riters.cpu().numpy()
 
+    def parity(self, data, limit=512):
+        """Oracle figures on the first `limit` instances (the oracle takes ~50 ms
+        per large instance on one core)."""
+        from oracle import parity
+        from qpax_b200.packed import unpack
+
+        k = min(limit, self.spec.batch)
+        L = self.plan.lengths
+        cut = lambda t, f: [v.cpu().numpy() for v in unpack(t, L[f])[:k]]
+        sub = [v[:k] for v in data]
+        fig = parity.standard(sub, self.spec.tol, KAPPA, cut(self.gx, 1), cut(self.out[0], 1),
+                              self.out[4][:k].cpu().numpy(), self.out[5][:k].cpu().numpy(),
+                              [cut(self.grads[f], f) for f in range(6)])[0]
+        fig["sample"] = f"the first {k} instances of the batch"
+        return fig
+
     def kernel_name(self, which):
-        return (f"qpb_solve_qp_packed: {self.plan.num_bins} size-bin kernels, concurrent (forward)"
+        return (f"qpb_solve_qp_packed: {self.plan.num_bins} size-bin kernels, concurrent, CUDA graph (forward)"
                 if which == "forward" else
-                f"qpb_solve_qp_primal_bwd_packed: {self.plan.num_bins} size-bin kernels, concurrent (backward)")
+                f"qpb_solve_qp_primal_bwd_packed: {self.plan.num_bins} size-bin kernels, concurrent, CUDA graph "
+                "(backward)")
 
 
 ARMS = {"uniform": UniformArm, "elastic": ElasticArm, "uneven": UnevenArm}
@@ -462,6 +520,40 @@ def variants_for(spec: Spec):
         v["fp64_cta"] = dict(precision="fp64", team_threads=128)  # plain FP64, one QP per CTA
     v["mixed"] = dict(precision="mixed")                          # FP32 factor + FP64 refinement
     return v
+
+
+VARIANT_NAMES = {"auto": "default", "fp64_cta": "fp64_one_cta_per_qp", "mixed": "mixed_fp32_factor_fp64_refinement"}
+
+
+def time_arm(args, arm, stream, flush, world, steps, sampler=None):
+    """W warm-up steps, then `steps` timed steps (forward, backward), L2 flushed
+    between steps outside the per-step events; device time, max over ranks."""
+    import torch
+
+    for _ in range(args.warmup):
+        arm.fwd()
+        arm.bwd()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__enter__()
+    for k in range(steps):
+        flush.fill_(float(k))
+        evs[k][0].record(stream)
+        arm.fwd()
+        evs[k][1].record(stream)
+        arm.bwd()
+        evs[k][2].record(stream)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    barrier(world)
+    fwd_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    bwd_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    tot = barrier_max(sum(f + b for f, b in zip(fwd_ms, bwd_ms)), world)
+    return tot, float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
 
 
 def run_ours(args, spec: Spec, world, rank, local):
@@ -481,36 +573,17 @@ def run_ours(args, spec: Spec, world, rank, local):
     arm_main = None
     for prec, opts in variants.items():
         arm = ARMS[spec.kind](spec, data, dev, opts)
-        for _ in range(args.warmup):
-            arm.fwd()
-            arm.bwd()
-        torch.cuda.synchronize()
-        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
-        barrier(world)
-        torch.cuda.synchronize()
         sampler = ClockSampler(local) if prec == "auto" else None
-        if sampler:
-            sampler.__enter__()
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            evs[k][0].record(stream)
-            arm.fwd()
-            evs[k][1].record(stream)
-            arm.bwd()
-            evs[k][2].record(stream)
-        torch.cuda.synchronize()
-        if sampler:
-            sampler.__exit__(None, None, None)
-        barrier(world)
-        fwd_ms = [e[0].elapsed_time(e[1]) for e in evs]
-        bwd_ms = [e[1].elapsed_time(e[2]) for e in evs]
-        tot = barrier_max(sum(f + b for f, b in zip(fwd_ms, bwd_ms)), world)
+        tot, fwd_ms, bwd_ms = time_arm(args, arm, stream, flush, world, args.steps, sampler)
         conv, iters, riters = arm.counts()
-        results[prec] = dict(total_ms=tot, fwd_ms=float(np.mean(fwd_ms)), bwd_ms=float(np.mean(bwd_ms)),
-                             conv=conv, iters=iters, riters=riters, clocks=sampler.summary() if sampler else None)
+        par = arm.parity(data) if (rank == 0 and not args.no_parity) else None
+        results[prec] = dict(total_ms=tot, fwd_ms=fwd_ms, bwd_ms=bwd_ms, conv=conv, iters=iters, riters=riters,
+                             clocks=sampler.summary() if sampler else None, parity=par)
         if prec == "auto":
             arm_main = arm
         else:
+            if hasattr(arm, "release"):
+                arm.release()
             del arm
 
     B = spec.batch
@@ -526,10 +599,11 @@ def run_ours(args, spec: Spec, world, rank, local):
     simt = simt_peaks()
     traffic = load_traffic(spec)
     roof = {
-        "bound": "tensor", "kernel": arm_main.kernel_name(dom_key), "achieved": achieved, "unit": "TFLOP/s",
+        "bound": "fp64", "kernel": arm_main.kernel_name(dom_key), "achieved": achieved, "unit": "TFLOP/s",
         "peak": peaks["bf16_tflops"], "frac": achieved / peaks["bf16_tflops"],
-        "peak_source": f"bf16 dense tensor peak of MEASURED_PEAKS.json ({peak_src}); the kernel is FP64 "
-                       "arithmetic, so its own roof is the FP64 FMA peak below",
+        "peak_source": f"bf16 dense tensor peak of MEASURED_PEAKS.json ({peak_src}), the figure the benchmark "
+                       "contract names; the kernel computes in FP64 (FMA pipe and FP64 tensor-core DMMA), whose "
+                       "own roof is fp64_fma_peak",
         "fp64_fma_peak": simt["fp64_tflops"], "frac_of_fp64_fma_peak": achieved / simt["fp64_tflops"],
         "fp32_fma_peak": simt["fp32_tflops"], "fma_peak_source": simt["how"],
         "algorithmic_flops_per_launch": fl[dom_key], "avg_launch_ms": dom_ms,
@@ -556,36 +630,80 @@ def run_ours(args, spec: Spec, world, rank, local):
     }
     if len(results) > 1:
         v = {k: world * B * args.steps / (r["total_ms"] * 1e-3) for k, r in results.items()}
-        names = {"fp64_cta": "fp64_one_cta_per_qp", "mixed": "mixed_fp32_factor_fp64_refinement"}
-        line["variants"] = {names[k]: {"value": v[k], "unit": "QPs/s", "ms_per_step": results[k]["total_ms"] /
-                                       args.steps} for k in results if k != "auto"}
+        line["variants"] = {VARIANT_NAMES[k]: {"value": v[k], "unit": "QPs/s", "ms_per_step": results[k]["total_ms"] /
+                                               args.steps} for k in results if k != "auto"}
         plain = "fp64_cta" if "fp64_cta" in v else "auto"
         if "mixed" in v:
             line["mixed_over_plain_fp64"] = v["mixed"] / v[plain]
         line["default_over_plain_fp64"] = v["auto"] / v[plain]
-        line["converged_flags_identical"] = bool(all((r["conv"] == main_r["conv"]).all() for r in results.values()))
-        line["iteration_counts_identical"] = bool(all((r["iters"] == main_r["iters"]).all()
-                                                      for r in results.values()))
+    if rank == 0 and not args.no_parity:
+        line["parity"] = {VARIANT_NAMES[k]: r["parity"] for k, r in results.items()}
+        line["parity"]["against"] = ("the FP64 oracle (C restatement of qpax) on the same inputs and the same dl/dx, "
+                                     "computed after the timed steps; errors relative per instance, "
+                                     "||gpu - ref||_inf / max(1, ||ref||_inf); objective 1/2 x'Qx + q'x")
     if not args.no_e2e:  # every rank takes part (barriers, max over ranks)
         e2e = run_e2e(args, spec, data, dev, arm_main, world)
         if rank == 0:
             line["e2e"] = e2e
+    if hasattr(arm_main, "release"):
+        arm_main.release()
+    del arm_main
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(spec, data)
+    if spec.key == "dense" and not args.no_configs:
+        line["configs"] = run_configs(args, world, rank, dev, stream, flush)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def simt_peaks():
-    """FP32 / FP64 FMA throughput of this GPU, measured with a dependent-chain-free FMA loop."""
+def run_configs(args, world, rank, dev, stream, flush):
+    """The other four configurations on the default path, each with its own
+    device-timed value, end-to-end value from host buffers and parity against
+    the oracle (uneven: on its first 512 instances)."""
     import torch
 
-    from qpax_b200 import _lib
+    out = {}
+    for key in ("nnls", "small", "uneven", "elastic"):
+        spec = WORKLOADS[key]
+        data = make_data(spec)
+        arm = ARMS[spec.kind](spec, data, dev, dict(precision="auto"))
+        steps = args.config_steps
+        tot, fwd_ms, bwd_ms = time_arm(args, arm, stream, flush, world, steps)
+        conv, iters, riters = arm.counts()
+        entry = {"workload": spec.workload, "metric": metric_for(spec),
+                 "value": world * spec.batch * steps / (tot * 1e-3), "unit": "QPs/s", "steps": steps,
+                 "ms_per_step": tot / steps, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                 "iterations": {"forward_mean": float(iters.mean()), "relax_mean": float(riters.mean()),
+                                "converged": float(conv.mean())},
+                 "gpu_launches": arm.launches * steps}
+        if rank == 0 and not args.no_parity:
+            entry["parity"] = arm.parity(data)
+        if not args.no_e2e:
+            sub = argparse.Namespace(**vars(args))
+            sub.steps = steps
+            sub.e2e_chunks = E2E_CHUNKS[key]
+            e2e = run_e2e(sub, spec, data, dev, arm, world)
+            if rank == 0:
+                entry["e2e"] = e2e
+        if hasattr(arm, "release"):
+            arm.release()
+        del arm, data
+        torch.cuda.empty_cache()
+        out[key] = entry
+    return out
 
-    lib = _lib.load()
-    fn = getattr(lib, "qpb_bench_fma_peak", None)
-    if fn is None:
-        return {"fp32_tflops": 75.0, "fp64_tflops": 37.0, "how": "nominal (no microbenchmark in the library)"}
+
+def simt_peaks():
+    """FP32 / FP64 FMA throughput of this GPU: independent FMA chains in every
+    thread of a full grid (libqpb_peak.so, the benchmark's own helper library;
+    the driver measures no FP64 figure)."""
+    import torch
+
+    path = os.path.join(ROOT, "qpax_b200", "libqpb_peak.so")
+    if not os.path.exists(path):
+        return {"fp32_tflops": 75.0, "fp64_tflops": 37.0, "how": "nominal (libqpb_peak.so not built)"}
+    lib = ctypes.CDLL(path)
+    fn = lib.qpb_bench_fma_peak
     fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     fn.restype = ctypes.c_double
     out = {}
@@ -595,10 +713,16 @@ def simt_peaks():
         for _ in range(3):
             best = max(best, fn(prec, buf.data_ptr(), torch.cuda.current_stream().cuda_stream))
         out[key] = best
-    out["how"] = "qpb_bench_fma_peak, best of 3"
+    out["how"] = "FMA-chain microbenchmark (libqpb_peak.so, not part of libqpb.so), best of 3, this run"
     if not (out["fp32_tflops"] > 0 and out["fp64_tflops"] > 0):
         return {"fp32_tflops": 75.0, "fp64_tflops": 37.0, "how": "nominal (microbenchmark failed)"}
     return out
+
+
+# slices of the host-buffer pipelines: copies of the large workloads overlap
+# best in 4-8 slices; small ones want few (each slice's launch must still fill
+# the GPU)
+E2E_CHUNKS = {"dense": 4, "nnls": 4, "small": 2, "uneven": 8, "elastic": 1}
 
 
 def run_e2e(args, spec: Spec, data, dev, arm, world=1):
@@ -690,12 +814,14 @@ def main():
                     help="slices of the host-buffer pipeline (0: the workload's setting, measured best)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity figures")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="dense workload: skip the other four configurations' block")
+    ap.add_argument("--config-steps", type=int, default=5, help="timed steps of each configuration in the block")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
     if args.e2e_chunks <= 0:
-        # copies of the large workloads overlap best in 4-8 slices; small
-        # ones want few slices (each slice's launch must still fill the GPU)
-        args.e2e_chunks = {"dense": 4, "nnls": 4, "small": 2, "uneven": 8, "elastic": 1}[spec.key]
+        args.e2e_chunks = E2E_CHUNKS[spec.key]
     if args.batch > 0 and args.batch != spec.batch:
         spec = Spec(spec.key, spec.kind, args.batch, spec.n, spec.m, spec.p, spec.tol,
                     spec.workload.replace(f"{spec.batch}", f"{args.batch}", 1))

@@ -20,6 +20,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqpb.so")
+# the benchmark's FMA-throughput helper: a library of its own, not product code
+PEAK_SOURCES = ["qpb_peak.cu"]
+PEAK_LIB = os.path.join(HERE, "libqpb_peak.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = [
@@ -29,7 +32,6 @@ SOURCES = [
     "qpb_kern_elastic_f64.cu",
     "qpb_kern_elastic_mixed.cu",
     "qpb_kern_warp.cu",
-    "qpb_bench.cu",
     "qpb_noalloc.cu",
     "qpb_plan.cu",
     "qpb_host_pipeline.cu",
@@ -64,18 +66,25 @@ def _compile(src: str, force: bool, extra: list[str]) -> str:
     return obj
 
 
-def build(force: bool = False, jobs: int | None = None, extra: list[str] | None = None) -> str:
-    """Compile every CUDA translation unit for sm_100a and link libqpb.so."""
-    os.makedirs(OBJ, exist_ok=True)
-    extra = list(extra or [])
-    jobs = jobs or min(len(SOURCES), os.cpu_count() or 1)
-    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        objs = list(ex.map(lambda s: _compile(s, force, extra), SOURCES))
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
+def _link(lib: str, objs: list[str], force: bool) -> None:
+    if force or not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+
+
+def build(force: bool = False, jobs: int | None = None, extra: list[str] | None = None) -> str:
+    """Compile every CUDA translation unit for sm_100a and link libqpb.so (and
+    the benchmark's libqpb_peak.so)."""
+    os.makedirs(OBJ, exist_ok=True)
+    extra = list(extra or [])
+    srcs = SOURCES + PEAK_SOURCES
+    jobs = jobs or min(len(srcs), os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(lambda s: _compile(s, force, extra), srcs))
+    _link(LIB, objs[: len(SOURCES)], force)
+    _link(PEAK_LIB, objs[len(SOURCES):], force)
     return LIB
 
 

@@ -1,7 +1,8 @@
-// qpb_bench.cu -- FMA throughput microbenchmark (include/qpb_bench.h).
+// qpb_peak.cu -- FMA throughput microbenchmark (qpb_peak.h), built as its own
+// library (libqpb_peak.so) for the benchmark; not part of libqpb.so.
 #include <cuda_runtime.h>
 
-#include "../../include/qpb_bench.h"
+#include "qpb_peak.h"
 
 namespace {
 

@@ -1,10 +1,10 @@
 /*
- * qpb_bench.h -- measurement helper exported by libqpb.so (no counterpart in
- * qpax: it exists to put the solver's FP32/FP64 arithmetic next to the
- * throughput the GPU can deliver).
+ * qpb_peak.h -- measurement helper of libqpb_peak.so, a library of its own
+ * that only the benchmark loads (no counterpart in qpax: it puts the solver's
+ * FP32/FP64 arithmetic next to the throughput the GPU can deliver).
  */
-#ifndef QPB_BENCH_H_
-#define QPB_BENCH_H_
+#ifndef QPB_PEAK_H_
+#define QPB_PEAK_H_
 
 #ifdef __cplusplus
 extern "C" {
@@ -21,4 +21,4 @@ double qpb_bench_fma_peak(int precision, void* scratch, void* stream);
 }
 #endif
 
-#endif /* QPB_BENCH_H_ */
+#endif /* QPB_PEAK_H_ */

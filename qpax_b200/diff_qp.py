@@ -33,7 +33,9 @@ class _SolveQPPrimal(torch.autograd.Function):
         ctx.opts = opts
         ctx.tols = (solver_tol, target_kappa)
         ctx.save_for_backward(x, s, z, y)
-        ctx.shapes = [t.shape for t in (Q, q, A, b, G, h)]
+        # each gradient goes back with its input's shape, device and dtype
+        # (inputs may live on the host or another GPU: they are copied here)
+        ctx.metas = [(t.shape, t.device, t.dtype) for t in (Q, q, A, b, G, h)]
         return x if bt.batched else x[0]
 
     @staticmethod
@@ -42,7 +44,7 @@ class _SolveQPPrimal(torch.autograd.Function):
         x, s, z, y = ctx.saved_tensors
         g = as_f64(gx, bt.dev).reshape(bt.B, bt.n).contiguous()
         grads = diff_qp_from_forward(bt, x, s, z, y, g, *ctx.tols, ctx.opts)
-        out = [gr.reshape(shp) for gr, shp in zip(grads, ctx.shapes)]
+        out = [gr.reshape(shp).to(device=dev, dtype=dt) for gr, (shp, dev, dt) in zip(grads, ctx.metas)]
         return (*out, None, None, None)
 
 

@@ -138,7 +138,8 @@ class _SolveQPElasticPrimal(torch.autograd.Function):
              [ctypes.c_double(solver_tol)] + [ptr(t) for t in it] + [ptr(conv), ptr(iters)])
         ctx.bt, ctx.opts, ctx.tols = bt, opts, (solver_tol, target_kappa)
         ctx.save_for_backward(*it)
-        ctx.shapes = [t.shape for t in (Q, q, G, h)]
+        # each gradient goes back with its input's shape, device and dtype
+        ctx.metas = [(t.shape, t.device, t.dtype) for t in (Q, q, G, h)]
         return it[0] if bt.batched else it[0][0]
 
     @staticmethod
@@ -146,7 +147,8 @@ class _SolveQPElasticPrimal(torch.autograd.Function):
         bt = ctx.bt
         g = as_f64(gx, bt.dev).reshape(bt.B, bt.n).contiguous()
         grads = _elastic_bwd(bt, list(ctx.saved_tensors), g, *ctx.tols, ctx.opts)
-        return (*[gr.reshape(s) for gr, s in zip(grads, ctx.shapes)], None, None, None, None)
+        out = [gr.reshape(shp).to(device=dev, dtype=dt) for gr, (shp, dev, dt) in zip(grads, ctx.metas)]
+        return (*out, None, None, None, None)
 
 
 def solve_qp_elastic_primal(Q, q, G, h, penalty, solver_tol: float = 1e-5, target_kappa: float = 1e-3, *,

@@ -1,0 +1,151 @@
+"""GPU parity on the five benchmark configurations exactly as seeded and
+benchmarked, on every instance, through every precision variant.
+
+Each case runs the benchmarked call (forward solve + solve_qp_primal backward,
+or the elastic pair) on the full seeded batch -- the uneven configuration on
+its first 512 instances, which span n = 4..256 -- and compares with the FP64
+oracle (the restatement of qpax pinned by test_oracle.py):
+
+  converged flags:   identical on EVERY instance (no mask), including those
+                     where qpax's own method does not converge
+  iteration counts:  identical on every instance (forward)
+  x (elastic: x, t, s1, s2), objective:  <= 1e-6 relative per instance
+  gradients:         <= 1e-5 relative per instance and array
+                     (elastic: 1e-4; the relaxation of qpax's elastic VJP
+                     runs to its iteration cap, see test_gpu_parity.py)
+both compared where both sides converged.  Relative error of an array:
+||gpu - ref||_inf / max(1, ||ref||_inf).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle, parity
+from qpax_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = {
+    "auto": dict(precision="auto"),
+    "fp64-cta": dict(precision="fp64", team_threads=128),
+    "mixed": dict(precision="mixed"),
+}
+X_TOL, G_TOL, E_G_TOL = 1e-6, 1e-5, 1e-4
+KAPPA = 1e-3
+_REF = {}
+_DL = {}
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from qpax_b200 import _lib as L
+
+    L.load()
+
+
+def np_(t):
+    return t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+def _dl(name, data, tol):
+    """Incoming gradient of ||x - 1||^2 at the oracle's x, given to both sides."""
+    if name not in _DL:
+        x = oracle.solve_qp(*data, solver_tol=tol)[0]
+        _DL[name] = [wl.loss_grad(v) for v in x] if isinstance(x, list) else wl.loss_grad(x)
+    return _DL[name]
+
+
+def _uniform(name, data, tol, prec):
+    import qpax_b200 as qb
+    from qpax_b200.diff_qp import diff_qp_from_forward
+    from qpax_b200.pdip import StdBatch
+
+    opts = VARIANTS[prec]
+    dl = _dl(name, data, tol)
+    x, s, z, y, conv, iters = qb.solve_qp(*data, tol, **opts)
+    bt = StdBatch(*data)
+    gx = torch.tensor(dl, device=bt.dev)
+    grads = diff_qp_from_forward(bt, x, s, z, y, gx, tol, KAPPA, opts)
+    torch.cuda.synchronize()
+    fig, ref = parity.standard(data, tol, KAPPA, dl, np_(x), np_(conv), np_(iters), [np_(g) for g in grads],
+                               ref=_REF.get(name))
+    _REF[name] = ref
+    return fig
+
+
+def _check(fig, g_tol=G_TOL):
+    print(fig)
+    assert fig["conv_mismatch"] == 0, fig
+    assert fig["iters_mismatch"] == 0, fig
+    assert fig["max_err_x"] <= X_TOL, fig
+    assert fig["max_err_obj"] <= X_TOL, fig
+    assert fig["max_err_grad"] <= g_tol, fig
+
+
+@pytest.mark.parametrize("prec", list(VARIANTS))
+def test_nnls_10000(prec):
+    """Configuration 1: 10000 NNLS QPs (n = 5), tol 1e-6."""
+    _check(_uniform("nnls", wl.nnls(10000), 1e-6, prec))
+
+
+@pytest.mark.parametrize("prec", list(VARIANTS))
+def test_dense_4096(prec):
+    """Configuration 2 (the headline): 4096 dense QPs n = 32, m = 8, p = 64, tol 1e-6."""
+    _check(_uniform("dense", wl.config2(4096), 1e-6, prec))
+
+
+@pytest.mark.parametrize("prec", list(VARIANTS))
+def test_differentiation_2048(prec):
+    """Configuration 3: 2048 QPs n = 16, m = 4, p = 32, tol 1e-5."""
+    _check(_uniform("small", wl.config3(2048), 1e-5, prec))
+
+
+@pytest.mark.parametrize("prec", ["auto", "mixed"])
+def test_uneven_first_512(prec):
+    """Configuration 4: the first 512 instances of the seeded uneven batch
+    (n ~ U{4..256}, p = 2n, m ~ U{0..n/4}) in one packed call, forward and
+    backward, every instance's converged flag against the oracle."""
+    from qpax_b200.packed import PackedPlan, pack, unpack
+
+    data = [v[:512] for v in wl.uneven(16384)]
+    assert max(len(q) for q in data[1]) > 128
+    shapes = [(len(q), len(b), len(h)) for q, b, h in zip(data[1], data[3], data[5])]
+    plan = PackedPlan(shapes, precision=VARIANTS[prec]["precision"])
+    ins = [pack(v) for v in data]
+    dl = _dl("uneven", data, 1e-6)
+    x, s, z, y, conv, iters = plan.solve(*ins, 1e-6)
+    grads = plan.primal_bwd(*ins, x, s, z, y, pack(dl), 1e-6, KAPPA)
+    torch.cuda.synchronize()
+    L = plan.lengths
+    x_list = [np_(t) for t in unpack(x, L[1])]
+    g_lists = [[np_(t) for t in unpack(grads[k], L[k])] for k in range(6)]
+    fig, ref = parity.standard(data, 1e-6, KAPPA, dl, x_list, np_(conv), np_(iters), g_lists,
+                               ref=_REF.get("uneven"))
+    _REF["uneven"] = ref
+    _check(fig)
+
+
+@pytest.mark.parametrize("prec", ["auto", "mixed"])
+def test_elastic_1024(prec):
+    """Configuration 5: 1024 elastic QPs n = 64, p = 128, penalty 1e3, 30 %
+    infeasible: x, t, s1, s2 and the four gradients."""
+    import qpax_b200 as qb
+    from qpax_b200.elastic_qp import ElasticBatch, _elastic_bwd
+
+    Q, q, G, h, _ = wl.elastic(1024)
+    opts = VARIANTS[prec]
+    if "elastic" not in _DL:
+        _DL["elastic"] = wl.loss_grad(oracle.solve_qp_elastic(Q, q, G, h, 1e3, solver_tol=1e-6)[0])
+    dl = _DL["elastic"]
+    out = qb.solve_qp_elastic(Q, q, G, h, 1e3, 1e-6, **opts)
+    bt = ElasticBatch(Q, q, G, h, 1e3)
+    grads = _elastic_bwd(bt, [t.contiguous() for t in out[:6]], torch.tensor(dl, device=bt.dev), 1e-6, KAPPA,
+                         opts)
+    torch.cuda.synchronize()
+    fig, ref = parity.elastic((Q, q, G, h), 1e3, 1e-6, KAPPA, dl, [np_(t) for t in out], [np_(g) for g in grads],
+                              ref=_REF.get("elastic"))
+    _REF["elastic"] = ref
+    _check(fig, E_G_TOL)
