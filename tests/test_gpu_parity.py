@@ -61,18 +61,20 @@ def assert_close(gpu, ref, tol, what):
 
 
 def check_solve(Q, q, A, b, G, h, tol, prec, max_breakdown=0.0, **kw):
-    """Parity on every instance qpax's method converges on.  Where the FP64
-    reference itself breaks down (its residual reaches ~tol, then grows until
-    the 30-iteration cap: ill-conditioned H late in the loop), the trajectory
-    after the breakdown is set by rounding and is not compared; the share of
-    such instances is bounded by max_breakdown."""
+    """Converged flags identical on every instance; outputs and iteration
+    counts compared on every instance qpax's method converges on.  Where the
+    FP64 reference itself breaks down (its residual reaches ~tol, then grows
+    until the 30-iteration cap: ill-conditioned H late in the loop), the GPU
+    must not converge either; the trajectory after the breakdown is set by
+    rounding and is not compared.  The share of such instances is bounded by
+    max_breakdown."""
     import qpax_b200 as qb
 
     out = qb.solve_qp(Q, q, A, b, G, h, tol, **VARIANTS[prec], **kw)
     ref = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=tol)
     ok = np.atleast_1d(ref[4]) == 1
     assert (~ok).mean() <= max_breakdown, f"reference breakdowns {(~ok).sum()} of {ok.size}"
-    np.testing.assert_array_equal(np.atleast_1d(np_(out[4]))[ok], 1, err_msg="converged flags")
+    np.testing.assert_array_equal(np.atleast_1d(np_(out[4])), np.atleast_1d(ref[4]), err_msg="converged flags")
     np.testing.assert_array_equal(np.atleast_1d(np_(out[5]))[ok], np.atleast_1d(ref[5])[ok],
                                   err_msg="iteration counts")
     for k, name in enumerate("xszy"):
@@ -420,3 +422,92 @@ def test_stats_count_factorisations():
     stats.zero_()
     qb.solve_qp(Q, q, A, b, G, h, 1e-6, precision="fp64", stats=stats)
     assert (np_(stats)[:, 0] == 0).all()
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", [(16, 4, 32), (32, 8, 64), (48, 12, 96)])
+def test_diff_qp_entry_point(prec, shape):
+    """qpb_diff_qp (qpax/diff_qp.py:20-46) as a standalone call at the
+    oracle's relaxed iterate: the six gradients vs the oracle's diff_qp."""
+    import qpax_b200 as qb
+
+    n, m, p = shape
+    Q, q, A, b, G, h = wl.dense(48, n, m, p, 600 + n)
+    x, s, z, y, conv, _ = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=1e-6)
+    xr, sr, zr, yr, rconv, _ = oracle.relax_qp(Q, q, A, b, G, h, x, s, z, y, solver_tol=1e-6, target_kappa=1e-3)
+    assert (conv == 1).all() and (rconv == 1).all()
+    dl = wl.loss_grad(xr)
+    grads = qb.diff_qp(Q, q, A, b, G, h, xr, sr, zr, yr, dl, **VARIANTS[prec])
+    grads_o = oracle.diff_qp(Q, q, A, b, G, h, xr, sr, zr, yr, dl)
+    for g, go, name in zip(grads, grads_o, ["dQ", "dq", "dA", "db", "dG", "dh"]):
+        assert_close(g, go, G_TOL, name)
+
+
+def _elastic_solved(seed, n, p, pen):
+    Q, q, G, h, _ = wl.elastic(24, seed=seed, n=n, p=p, pairs=2)
+    out = oracle.solve_qp_elastic(Q, q, G, h, pen, solver_tol=1e-6)
+    assert (out[6] == 1).all()
+    return (Q, q, G, h), out
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", [(12, 24), (64, 128)])
+def test_relax_qp_elastic_entry_point(prec, shape):
+    """qpb_relax_qp_elastic (qpax/elastic_qp.py:319-359) from the oracle's
+    elastic solution: all six relaxed variables, converged flags and
+    iteration counts vs the oracle's relax_qp_elastic.  (qpax's elastic
+    relaxation does not converge where t != 0 -- its residual signs,
+    elastic_qp.py:255-261 -- and runs to the 30-iteration cap there, on both
+    sides.)"""
+    import qpax_b200 as qb
+
+    n, p = shape
+    data, out = _elastic_solved(700 + n, n, p, 50.0)
+    got = qb.relax_qp_elastic(*data, 50.0, *out[:6], 1e-6, 1e-3, **VARIANTS[prec])
+    ref = oracle.relax_qp_elastic(*data, 50.0, *out[:6], solver_tol=1e-6, target_kappa=1e-3)
+    np.testing.assert_array_equal(np_(got[6]), ref[6])
+    np.testing.assert_array_equal(np_(got[7]), ref[7])
+    for k, name in enumerate(["x", "t", "s1", "s2", "z1", "z2"]):
+        assert_close(got[k], ref[k], X_TOL, name)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", [(12, 24), (64, 128)])
+def test_diff_qp_elastic_entry_point(prec, shape):
+    """qpb_diff_qp_elastic (qpax/elastic_qp.py:381-417) as a standalone call at
+    the oracle's relaxed elastic iterate: dQ, dq, dG, dh vs the oracle."""
+    import qpax_b200 as qb
+
+    n, p = shape
+    data, out = _elastic_solved(800 + n, n, p, 50.0)
+    rel = oracle.relax_qp_elastic(*data, 50.0, *out[:6], solver_tol=1e-6, target_kappa=1e-3)
+    dl = wl.loss_grad(rel[0])
+    grads = qb.diff_qp_elastic(*data, *rel[:6], dl, penalty=50.0, **VARIANTS[prec])
+    grads_o = oracle.diff_qp_elastic(*data, *rel[:6], dl)
+    for g, go, name in zip(grads, grads_o, ["dQ", "dq", "dG", "dh"]):
+        assert_close(g, go, G_TOL, name)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_nonsymmetric_Q_is_read_as_its_symmetric_part(prec):
+    """A non-symmetric Q: every entry point reads it as (Q + Q')/2, the matrix
+    the objective 1/2 x'Qx depends on.  qpax symmetrizes in solve_qp
+    (pdip.py:223) but relaxes and differentiates with the raw Q
+    (diff_qp.py:66-67, 76-79) -- a deviation documented with its measured
+    size; here the GPU forward must equal the oracle's on the raw Q (qpax's
+    own solve) and the GPU backward the oracle's on sym(Q)."""
+    import qpax_b200 as qb
+
+    Q, q, A, b, G, h = wl.dense(32, 16, 4, 32, 71)
+    K = np.random.default_rng(5).standard_normal(Q.shape)
+    Qn = Q + 1e-3 * (K - K.transpose(0, 2, 1)) * np.abs(Q).mean(axis=(1, 2), keepdims=True)
+    Qs = 0.5 * (Qn + Qn.transpose(0, 2, 1))
+    out = qb.solve_qp(Qn, q, A, b, G, h, 1e-6, **VARIANTS[prec])
+    ref = oracle.solve_qp(Qn, q, A, b, G, h, solver_tol=1e-6)
+    np.testing.assert_array_equal(np_(out[4]), ref[4])
+    assert_close(out[0], ref[0], X_TOL, "x (forward, raw Q)")
+    dl = wl.loss_grad(ref[0])
+    _, grads, _, _ = qb.solve_qp_primal_vjp(Qn, q, A, b, G, h, dl, 1e-6, 1e-3, **VARIANTS[prec])
+    _, grads_o, _, _ = oracle.solve_qp_primal_vjp(Qs, q, A, b, G, h, dl, solver_tol=1e-6, target_kappa=1e-3)
+    for g, go, name in zip(grads, grads_o, ["dQ", "dq", "dA", "db", "dG", "dh"]):
+        assert_close(g, go, G_TOL, name)

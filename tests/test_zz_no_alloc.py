@@ -75,6 +75,29 @@ def test_noalloc_matches_workspace_entry_point(lib, shape, cfg):
                 assert (np.abs(g - r) / scale).max() <= 1e-6, f"call {call}, output {k}"
 
 
+def test_noalloc_global_arena_within_scratch(lib):
+    """A plan whose instances live in global-memory arenas (FP64, n > 32, a
+    tiny batch) that still fits the 1 MiB array: the arena offsets inside the
+    array are exercised, and the outputs equal qpb_solve_qp's bit for bit, on
+    two calls in a row."""
+    import qpax_b200 as qb
+    from qpax_b200 import _lib as L
+    from qpax_b200 import workloads as wl
+
+    B, n, m, p = 2, 48, 6, 96
+    dims = L.Dims(B, n, m, p)
+    need = lib.qpb_workspace_size(0, ctypes.byref(dims), None)
+    assert 256 < need <= (1 << 20), need
+    for call, seed in enumerate((303, 404)):
+        data = [torch.tensor(a, device="cuda") for a in wl.dense(B, n, m, p, seed)]
+        ref = qb.solve_qp(*data, 1e-6)
+        st, out = _noalloc(lib, *data, 1e-6)
+        torch.cuda.synchronize()
+        assert st == 0, f"call {call}: status {st}"
+        for k in range(6):
+            np.testing.assert_array_equal(out[k].cpu().numpy(), ref[k].cpu().numpy(), err_msg=f"call {call}, {k}")
+
+
 def test_noalloc_refuses_problems_beyond_its_scratch(lib):
     from qpax_b200 import workloads as wl
 
