@@ -90,6 +90,23 @@ int qpb_solve_qp(const qpb_dims* dims, const double* Q, const double* q, const d
                  int32_t* converged, int32_t* iters, const qpb_config* cfg, void* workspace,
                  size_t workspace_bytes, qpb_stream_t stream);
 
+/* Autotuned solve_qp (no qpax counterpart; it stands where qpax compiles one
+ * jit(vmap) per shape, qpax/pdip.py:208-217): times the launch shapes the
+ * kernels support for `dims` -- threads per instance, arena placement, G
+ * chunk rows, resident CTAs per SM -- on the first instances of this batch
+ * (about two waves each; the host waits on `stream`), records the fastest
+ * per instance for these (n, m, p) on this device, then solves the whole
+ * batch with it; later qpb_solve_qp / qpb_workspace_size calls with these
+ * (n, m, p) and automatic team_threads use the recorded shape.  Arguments
+ * and outputs as qpb_solve_qp; `workspace` must hold
+ * qpb_tune_workspace_size(QPB_OP_SOLVE, dims, cfg) bytes. */
+int qpb_tune_solve_qp(const qpb_dims* dims, const double* Q, const double* q, const double* A, const double* b,
+                      const double* G, const double* h, double solver_tol, double* x, double* s, double* z,
+                      double* y, int32_t* converged, int32_t* iters, const qpb_config* cfg, void* workspace,
+                      size_t workspace_bytes, qpb_stream_t stream);
+/* Workspace bytes of the autotuned calls (the largest candidate's). */
+size_t qpb_tune_workspace_size(int32_t op, const qpb_dims* dims, const qpb_config* cfg);
+
 /* qpax/pdip.py:15-35 initialize(Q, q, A, b, G, h) -> (x, s, z, y), on the data as given. */
 int qpb_initialize(const qpb_dims* dims, const double* Q, const double* q, const double* A, const double* b,
                    const double* G, const double* h, double* x, double* s, double* z, double* y,
@@ -130,6 +147,15 @@ int qpb_solve_qp_elastic(const qpb_dims* dims, const double* Q, const double* q,
                          const double* h, const double* penalty, double solver_tol, double* x, double* t,
                          double* s1, double* s2, double* z1, double* z2, int32_t* converged, int32_t* iters,
                          const qpb_config* cfg, void* workspace, size_t workspace_bytes, qpb_stream_t stream);
+
+/* Autotuned solve_qp_elastic: as qpb_tune_solve_qp, for the elastic entry
+ * points (the recorded shape serves every elastic op with these dims);
+ * workspace: qpb_tune_workspace_size(QPB_OP_ELASTIC_SOLVE, dims, cfg). */
+int qpb_tune_solve_qp_elastic(const qpb_dims* dims, const double* Q, const double* q, const double* G,
+                              const double* h, const double* penalty, double solver_tol, double* x, double* t,
+                              double* s1, double* s2, double* z1, double* z2, int32_t* converged, int32_t* iters,
+                              const qpb_config* cfg, void* workspace, size_t workspace_bytes,
+                              qpb_stream_t stream);
 
 /* qpax/elastic_qp.py:27-47 initialize_elastic -> (x, t, s1, s2, z1, z2). */
 int qpb_initialize_elastic(const qpb_dims* dims, const double* Q, const double* q, const double* G,
@@ -181,6 +207,31 @@ size_t qpb_plan_workspace_size(const qpb_plan* plan);
 int32_t qpb_plan_num_bins(const qpb_plan* plan);
 /* Packed lengths (elements) of Q, q, A, b, G, h. */
 int qpb_plan_totals(const qpb_plan* plan, int64_t totals[6]);
+
+/* Size-bin autotuner.  Replaces qpax's per-shape compilation
+ * (qpax/pdip.py:208-217: one jit(vmap) per shape, each traced and compiled
+ * by XLA) with a per-bin search of launch shapes: threads per instance (one
+ * warp, 128 or 256), arena placement (shared or global memory), rows of G
+ * per shared-memory chunk and resident CTAs per SM.  Each candidate the
+ * kernels support for the bin's dims runs the forward solve on the bin's
+ * heaviest instances (about two waves) on `stream`, timed with events (the
+ * host waits); the fastest per instance becomes the bin's launch shape and
+ * is recorded for this device, so later plans -- and uniform calls -- whose
+ * bin has the same largest (n, m, p) start from it.  The whole batch is then
+ * solved with the tuned plan: outputs as qpb_solve_qp_packed.  Plans created
+ * with cfg->team_threads != 0 keep their launch shape (the call only
+ * solves).  The plan's workspace size may change: query
+ * qpb_plan_workspace_size again afterwards.  `workspace` must hold
+ * qpb_plan_tune_workspace_size(plan) bytes. */
+size_t qpb_plan_tune_workspace_size(const qpb_plan* plan);
+int qpb_plan_tune(qpb_plan* plan, const double* Q, const double* q, const double* A, const double* b,
+                  const double* G, const double* h, double solver_tol, double* x, double* s, double* z, double* y,
+                  int32_t* converged, int32_t* iters, void* workspace, size_t workspace_bytes,
+                  qpb_stream_t stream);
+/* Launch shape of bin `bin` (0 .. num_bins - 1, launch order): info =
+ * {instances, n_max, m_max, p_max, threads per instance, arena placement
+ * (1 shared, 2 global memory), G chunk rows, resident CTAs per SM}. */
+int32_t qpb_plan_bin_info(const qpb_plan* plan, int32_t bin, int32_t info[8]);
 
 /* qpax/pdip.py:181-251 solve_qp over a packed batch (outputs packed like q, h, h, b). */
 int qpb_solve_qp_packed(const qpb_plan* plan, const double* Q, const double* q, const double* A, const double* b,

@@ -14,11 +14,11 @@ runs in libqpb.so (include/qpb.h); there is no CPU path.
 
 from .diff_qp import diff_qp, solve_qp_primal, solve_qp_primal_vjp, solve_qp_primal_vjp_host
 from .elastic_qp import (diff_qp_elastic, initialize_elastic, relax_qp_elastic, solve_qp_elastic,
-                         solve_qp_elastic_primal, solve_qp_elastic_primal_vjp)
-from .pdip import initialize, relax_qp, set_defaults, solve_qp
+                         solve_qp_elastic_primal, solve_qp_elastic_primal_vjp, tune_solve_qp_elastic)
+from .pdip import initialize, relax_qp, set_defaults, solve_qp, tune_solve_qp
 
 __all__ = [
     "solve_qp", "solve_qp_primal", "solve_qp_elastic", "solve_qp_elastic_primal", "initialize", "relax_qp",
     "diff_qp", "solve_qp_primal_vjp", "initialize_elastic", "relax_qp_elastic", "diff_qp_elastic",
-    "solve_qp_elastic_primal_vjp", "set_defaults",
+    "solve_qp_elastic_primal_vjp", "set_defaults", "tune_solve_qp", "tune_solve_qp_elastic",
 ]

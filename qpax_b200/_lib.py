@@ -56,6 +56,8 @@ _SIGS = {
     "qpb_relax_qp_elastic": "dims P P P P P A6 D D A6 P P cfg P S stream",
     "qpb_diff_qp_elastic": "dims P P P P P A6 P P P P P cfg P S stream",
     "qpb_solve_qp_elastic_primal_bwd": "dims P P P P P A6 P D D P P P P cfg P S stream",
+    "qpb_tune_solve_qp": "dims P P P P P P D P P P P P P cfg P S stream",
+    "qpb_tune_solve_qp_elastic": "dims P P P P P D P P P P P P P P cfg P S stream",
     "qpb_solve_qp_primal_vjp_host": "dims P P P P P P P D D P P P P P P P P P I cfg P S stream",
 }
 _CT = {
@@ -78,6 +80,8 @@ def load() -> ctypes.CDLL:
                 fn.restype = ctypes.c_int
             lib.qpb_workspace_size.argtypes = [ctypes.c_int32, ctypes.POINTER(Dims), ctypes.POINTER(Config)]
             lib.qpb_workspace_size.restype = ctypes.c_size_t
+            lib.qpb_tune_workspace_size.argtypes = [ctypes.c_int32, ctypes.POINTER(Dims), ctypes.POINTER(Config)]
+            lib.qpb_tune_workspace_size.restype = ctypes.c_size_t
             lib.qpb_solve_qp_primal_vjp_host_workspace_size.argtypes = [ctypes.POINTER(Dims), ctypes.c_int32,
                                                                         ctypes.POINTER(Config)]
             lib.qpb_solve_qp_primal_vjp_host_workspace_size.restype = ctypes.c_size_t
@@ -89,7 +93,7 @@ def load() -> ctypes.CDLL:
 
 
 def exported_symbols() -> list[str]:
-    return ["qpb_workspace_size", "qpb_status_string", "qpb_version",
+    return ["qpb_workspace_size", "qpb_tune_workspace_size", "qpb_status_string", "qpb_version",
             "qpb_solve_qp_primal_vjp_host_workspace_size"] + list(_SIGS)
 
 
@@ -119,9 +123,10 @@ def make_config(precision: str = "auto", team_threads: int = 0, pivot_max: float
     return Config(PRECISION[precision], team_threads, pivot_max, max_sweeps, ptr(stats))
 
 
-def workspace(op: str, dims: Dims, cfg: Config, dev: torch.device) -> torch.Tensor:
+def workspace(op: str, dims: Dims, cfg: Config, dev: torch.device, tune: bool = False) -> torch.Tensor:
     lib = load()
-    nbytes = lib.qpb_workspace_size(OPS[op], ctypes.byref(dims), ctypes.byref(cfg))
+    size = lib.qpb_tune_workspace_size if tune else lib.qpb_workspace_size
+    nbytes = size(OPS[op], ctypes.byref(dims), ctypes.byref(cfg))
     if nbytes == 0:
         raise QpbError(f"unsupported problem for {op}: batch={dims.batch} n={dims.n} m={dims.m} p={dims.p}")
     return torch.empty(int(nbytes) + 256, dtype=torch.uint8, device=dev)

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <vector>
 
 #include "../../include/qpb.h"
 #include "qpb_host.h"
@@ -54,6 +55,11 @@ static DevInfo dev_info() {
     cache[dev] = d;
   }
   return cache[dev];
+}
+
+int device_sms() {
+  const DevInfo d = dev_info();
+  return d.ok ? d.sms : 0;
 }
 
 // Per (device, kernel, block, shared memory): raises the kernel's dynamic
@@ -119,7 +125,51 @@ int warp_np(const qpb_dims& d) {
   return (np && d.m <= np / 4) ? np : 0;
 }
 
-int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
+// ------------------------------------------------------- tuned choices
+
+struct TuneEntry {
+  int dev, elastic, precision, n, m, p;
+  LaunchChoice ch;
+};
+static std::mutex g_tune_mu;
+static TuneEntry g_tune[512];
+static int g_tune_count = 0;
+
+void tune_record(int op, const qpb_dims& d, const qpb_config& cfg, const LaunchChoice& ch) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  const TuneEntry e{dev, op_is_elastic(op) ? 1 : 0, cfg.precision, d.n, d.m, d.p, ch};
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (int i = 0; i < g_tune_count; ++i) {
+    TuneEntry& t = g_tune[i];
+    if (t.dev == e.dev && t.elastic == e.elastic && t.precision == e.precision && t.n == e.n && t.m == e.m &&
+        t.p == e.p) {
+      t.ch = ch;
+      return;
+    }
+  }
+  if (g_tune_count < 512) g_tune[g_tune_count++] = e;
+}
+
+bool tune_lookup(int op, const qpb_dims& d, const qpb_config& cfg, LaunchChoice* ch) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  const int el = op_is_elastic(op) ? 1 : 0;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (int i = 0; i < g_tune_count; ++i) {
+    const TuneEntry& t = g_tune[i];
+    if (t.dev == dev && t.elastic == el && t.precision == cfg.precision && t.n == d.n && t.m == d.m &&
+        t.p == d.p) {
+      *ch = t.ch;
+      return true;
+    }
+  }
+  return false;
+}
+
+int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl, const LaunchChoice* ch) {
+  LaunchChoice tuned{};
+  if (!ch && cfg.team_threads == 0 && tune_lookup(op, d, cfg, &tuned)) ch = &tuned;
   const bool elastic = op_is_elastic(op);
   const bool mixed = cfg.precision == QPB_PRECISION_MIXED;
   const DevInfo di = dev_info();
@@ -127,7 +177,9 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   pl->gstage_rows = 0;
   const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
   const int np = warp_np(d);
-  if (!elastic && !mixed && np && (cfg.team_threads == 0 || cfg.team_threads == 32)) {
+  const int want_threads = ch && ch->team_threads ? ch->team_threads : cfg.team_threads;
+  const int cap = ch ? ch->per_sm_cap : 0;
+  if (!elastic && !mixed && np && (want_threads == 0 || want_threads == 32)) {
     // one warp per instance (n_pad = 16, 32) or four instances per warp in
     // lockstep (n_pad = 8), FP64, four warps per CTA; `teams` counts
     // instances per CTA
@@ -141,7 +193,9 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     pl->arena_bytes = arena;
     pl->teams = (kWarpKernelThreads / 32) * per_warp;
     pl->threads = kWarpKernelThreads;
-    if (arena * pl->teams <= smem_budget) {
+    const bool fits = arena * pl->teams <= smem_budget;
+    if (ch && ch->placement == 1 && !fits) return QPB_ERR_UNSUPPORTED;
+    if (fits && !(ch && ch->placement == 2)) {
       pl->in_smem = 1;
       pl->smem_bytes = arena * pl->teams;
     } else {
@@ -152,6 +206,7 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     if (occupancy(pl->fn, pl->threads, pl->smem_bytes, &per_sm) != QPB_OK) return QPB_ERR_CUDA;
     if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
     if (!pl->in_smem && per_sm > 4) per_sm = 4;
+    if (cap > 0 && per_sm > cap) per_sm = cap;
     const long need = ((long)d.batch + pl->teams - 1) / pl->teams;
     long grid = (long)per_sm * di.sms;
     grid = grid > need ? need : grid;
@@ -160,7 +215,7 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
     return QPB_OK;
   }
   const int KC = chunks_for(d.n > d.m ? d.n : d.m);
-  int NT = cfg.team_threads ? cfg.team_threads : auto_team(d.n, KC, mixed);
+  int NT = want_threads ? want_threads : auto_team(d.n, KC, mixed);
   if (NT == 32 && KC > 1) NT = 128;
   if (NT == 256 && KC < 4) NT = 128;
   KernelFn fn = pick_kernel(elastic, mixed, NT, KC);
@@ -191,9 +246,11 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   size_t gbytes = 0;
   if (NT > 32 && d.n > 32 && d.p > 0 && !mixed) {
     // stream G through shared memory in chunks of 32, 16 or 8 rows: the
-    // largest chunk among those that keep the most instances per SM
+    // largest chunk among those that keep the most instances per SM (or the
+    // tuned chunk)
     const int ldg = (d.n + 3) & ~3;
     for (int rows = 32; rows >= 8; rows >>= 1) {
+      if (ch && ch->gstage_rows && ch->gstage_rows != rows) continue;
       const size_t b = gstage_bytes(ldg, rows);
       if (b > team_budget) continue;
       int v = 0;
@@ -206,7 +263,14 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
       }
     }
   }
-  if (per_sm_smem >= 1 && per_sm_smem >= per_sm_global) {
+  bool use_smem = per_sm_smem >= 1 && per_sm_smem >= per_sm_global;
+  if (ch && ch->placement == 1) {
+    if (per_sm_smem < 1) return QPB_ERR_UNSUPPORTED;
+    use_smem = true;
+  } else if (ch && ch->placement == 2) {
+    use_smem = false;
+  }
+  if (use_smem) {
     pl->in_smem = 1;
     pl->teams = teams;
     pl->smem_bytes = arena * teams;
@@ -221,6 +285,7 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   if (occupancy(pl->fn, pl->threads, pl->smem_bytes, &per_sm) != QPB_OK) return QPB_ERR_CUDA;
   if (per_sm < 1) return QPB_ERR_UNSUPPORTED;
   if (!pl->in_smem && per_sm > 4) per_sm = 4;
+  if (cap > 0 && per_sm > cap) per_sm = cap;
   const long need = ((long)d.batch + pl->teams - 1) / pl->teams;
   long grid = (long)per_sm * di.sms;
   if (grid > need) grid = need;
@@ -228,6 +293,107 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl) {
   pl->grid = (int)grid;
   pl->ws_bytes = kCounterBytes + (pl->in_smem ? 0 : (size_t)grid * pl->teams * arena);
   return QPB_OK;
+}
+
+// Candidate launch shapes for the autotuner: the heuristic's own choice
+// first, then the team sizes, arena placements, G chunk rows and resident-CTA
+// caps (the occupancy limit and one below it) the kernels support for `d`.
+static std::vector<LaunchChoice> tune_candidates(int op, const qpb_dims& d, const qpb_config& c) {
+  std::vector<LaunchChoice> out;
+  out.push_back(LaunchChoice{});
+  const bool elastic = op_is_elastic(op);
+  const bool mixed = c.precision == QPB_PRECISION_MIXED;
+  const int KC = chunks_for(d.n > d.m ? d.n : d.m);
+  std::vector<int> teams;
+  if ((!elastic && !mixed && warp_np(d)) || KC == 1) teams.push_back(32);
+  teams.push_back(128);
+  if (KC >= 4) teams.push_back(256);
+  const int sms = device_sms();
+  for (int nt : teams) {
+    std::vector<LaunchChoice> shapes;
+    shapes.push_back(LaunchChoice{nt, 1, 0, 0});
+    if (nt > 32 && d.n > 32 && !mixed) {
+      for (int rows : {32, 16, 8}) shapes.push_back(LaunchChoice{nt, 2, rows, 0});
+    } else {
+      shapes.push_back(LaunchChoice{nt, 2, 0, 0});
+    }
+    for (const LaunchChoice& sh : shapes) {
+      Plan pl;
+      if (make_plan(op, d, c, &pl, &sh) != QPB_OK) continue;
+      const int per_sm = sms > 0 ? (pl.grid + sms - 1) / sms : 1;
+      for (int cap = per_sm; cap >= 1 && cap >= per_sm - 1; --cap) {
+        LaunchChoice ch = sh;
+        ch.per_sm_cap = cap;
+        out.push_back(ch);
+      }
+    }
+  }
+  return out;
+}
+
+size_t tune_workspace(int op, const qpb_dims& d, const qpb_config& cfg) {
+  size_t need = kCounterBytes;
+  for (const LaunchChoice& ch : tune_candidates(op, d, cfg)) {
+    Plan pl;
+    if (make_plan(op, d, cfg, &pl, &ch) == QPB_OK && pl.ws_bytes > need) need = pl.ws_bytes;
+  }
+  return need;
+}
+
+int tune_pick(Params P, int op, const qpb_dims& d, const qpb_config& cfg, void* ws, size_t ws_bytes,
+              qpb_stream_t stream, LaunchChoice* best) {
+  *best = LaunchChoice{};
+  if (d.batch == 0) return QPB_OK;
+  if (!ws || (reinterpret_cast<uintptr_t>(ws) & 255)) return QPB_ERR_WORKSPACE;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return QPB_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return QPB_ERR_CUDA;
+  }
+  int status = QPB_OK;
+  float best_per = 0.0f;
+  bool have = false;
+  P.n = d.n;
+  P.m = d.m;
+  P.p = d.p;
+  for (const LaunchChoice& ch : tune_candidates(op, d, cfg)) {
+    Plan pl;
+    if (make_plan(op, d, cfg, &pl, &ch) != QPB_OK || pl.ws_bytes > ws_bytes) continue;
+    // about two waves of the candidate's resident teams
+    long sample = 2L * pl.grid * pl.teams;
+    if (sample < 64) sample = 64;
+    if (sample > d.batch) sample = d.batch;
+    Params R = P;
+    R.batch = (int)sample;
+    R.counter = reinterpret_cast<int*>(ws);
+    R.arena = reinterpret_cast<unsigned char*>(ws) + kCounterBytes;
+    R.arena_bytes = pl.arena_bytes;
+    R.arena_in_smem = pl.in_smem;
+    R.gstage_rows = pl.gstage_rows;
+    const long need_teams = (sample + pl.teams - 1) / pl.teams;
+    const int grid = (int)(need_teams < pl.grid ? need_teams : pl.grid);
+    float ms = 0.0f;
+    for (int rep = 0; rep < 2 && status == QPB_OK; ++rep) {  // the first run warms the caches
+      void* args[] = {&R};
+      if (cudaMemsetAsync(ws, 0, sizeof(int), st) != cudaSuccess || cudaEventRecord(e0, st) != cudaSuccess ||
+          cudaLaunchKernel(pl.fn, dim3(grid), dim3(pl.threads), args, pl.smem_bytes, st) != cudaSuccess ||
+          cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+        status = QPB_ERR_CUDA;
+    }
+    if (status != QPB_OK) break;
+    const float per = ms / (float)sample;  // the candidates' samples differ in size
+    if (!have || per < best_per) {
+      have = true;
+      best_per = per;
+      *best = ch;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return status;
 }
 
 qpb_config resolve_config(const qpb_config* c) {
@@ -266,10 +432,23 @@ int check_common(int op, const qpb_dims* d, const qpb_config* cfg) {
   return QPB_OK;
 }
 
+// With `tune`, the launch shape is first chosen by timing the candidates
+// (tune_pick) and recorded for these dims on this device.
 static int launch(Params P, const qpb_dims* d, const qpb_config* cfg, void* ws, size_t ws_bytes,
-                  qpb_stream_t stream) {
+                  qpb_stream_t stream, bool tune = false) {
   const qpb_config c = resolve_config(cfg);
   if (d->batch == 0) return QPB_OK;
+  if (tune && c.team_threads == 0) {
+    Params T = P;
+    T.mixed = c.precision == QPB_PRECISION_MIXED;
+    T.pivot_max = c.pivot_max;
+    T.max_sweeps = c.max_sweeps;
+    T.stats = c.stats;
+    LaunchChoice best{};
+    const int st = tune_pick(T, P.op, *d, c, ws, ws_bytes, stream, &best);
+    if (st != QPB_OK) return st;
+    tune_record(P.op, *d, c, best);
+  }
   Plan pl;
   int st = make_plan(P.op, *d, c, &pl);
   if (st != QPB_OK) return st;
@@ -324,10 +503,14 @@ size_t qpb_workspace_size(int32_t op, const qpb_dims* dims, const qpb_config* cf
   return pl.ws_bytes;
 }
 
-int qpb_solve_qp(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
-                 const double* G, const double* h, double solver_tol, double* x, double* s, double* z, double* y,
-                 int32_t* converged, int32_t* iters, const qpb_config* cfg, void* ws, size_t ws_bytes,
-                 qpb_stream_t stream) {
+}  // extern "C"
+
+namespace qpb {
+
+static int solve_qp_impl(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                         const double* G, const double* h, double solver_tol, double* x, double* s, double* z,
+                         double* y, int32_t* converged, int32_t* iters, const qpb_config* cfg, void* ws,
+                         size_t ws_bytes, qpb_stream_t stream, bool tune) {
   int st = check_common(kOpSolve, d, cfg);
   if (st) return st;
   const long B = d->batch, n = d->n, m = d->m, p = d->p;
@@ -342,7 +525,33 @@ int qpb_solve_qp(const qpb_dims* d, const double* Q, const double* q, const doub
   P.out[0] = x; P.out[1] = s; P.out[2] = z; P.out[3] = y;
   P.conv = converged;
   P.iters = iters;
-  return launch(P, d, cfg, ws, ws_bytes, stream);
+  return launch(P, d, cfg, ws, ws_bytes, stream, tune);
+}
+
+}  // namespace qpb
+
+extern "C" {
+
+int qpb_solve_qp(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                 const double* G, const double* h, double solver_tol, double* x, double* s, double* z, double* y,
+                 int32_t* converged, int32_t* iters, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                 qpb_stream_t stream) {
+  return solve_qp_impl(d, Q, q, A, b, G, h, solver_tol, x, s, z, y, converged, iters, cfg, ws, ws_bytes, stream,
+                       false);
+}
+
+int qpb_tune_solve_qp(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
+                      const double* G, const double* h, double solver_tol, double* x, double* s, double* z,
+                      double* y, int32_t* converged, int32_t* iters, const qpb_config* cfg, void* ws,
+                      size_t ws_bytes, qpb_stream_t stream) {
+  return solve_qp_impl(d, Q, q, A, b, G, h, solver_tol, x, s, z, y, converged, iters, cfg, ws, ws_bytes, stream,
+                       true);
+}
+
+size_t qpb_tune_workspace_size(int32_t op, const qpb_dims* dims, const qpb_config* cfg) {
+  if (check_common(op, dims, cfg) != QPB_OK) return 0;
+  const qpb_config c = resolve_config(cfg);
+  return tune_workspace(op, *dims, c);
 }
 
 int qpb_initialize(const qpb_dims* d, const double* Q, const double* q, const double* A, const double* b,
@@ -458,10 +667,15 @@ static bool ok_iterate6(const qpb_dims* d, const double* const it[6]) {
   return true;
 }
 
-int qpb_solve_qp_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,
-                         const double* penalty, double solver_tol, double* x, double* t, double* s1, double* s2,
-                         double* z1, double* z2, int32_t* converged, int32_t* iters, const qpb_config* cfg,
-                         void* ws, size_t ws_bytes, qpb_stream_t stream) {
+}  // extern "C"
+
+namespace qpb {
+
+static int solve_qp_elastic_impl(const qpb_dims* d, const double* Q, const double* q, const double* G,
+                                 const double* h, const double* penalty, double solver_tol, double* x, double* t,
+                                 double* s1, double* s2, double* z1, double* z2, int32_t* converged,
+                                 int32_t* iters, const qpb_config* cfg, void* ws, size_t ws_bytes,
+                                 qpb_stream_t stream, bool tune) {
   int st = check_common(kOpESolve, d, cfg);
   if (st) return st;
   double* out[6] = {x, t, s1, s2, z1, z2};
@@ -475,7 +689,27 @@ int qpb_solve_qp_elastic(const qpb_dims* d, const double* Q, const double* q, co
   for (int k = 0; k < 6; ++k) P.out[k] = out[k];
   P.conv = converged;
   P.iters = iters;
-  return launch(P, d, cfg, ws, ws_bytes, stream);
+  return launch(P, d, cfg, ws, ws_bytes, stream, tune);
+}
+
+}  // namespace qpb
+
+extern "C" {
+
+int qpb_solve_qp_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,
+                         const double* penalty, double solver_tol, double* x, double* t, double* s1, double* s2,
+                         double* z1, double* z2, int32_t* converged, int32_t* iters, const qpb_config* cfg,
+                         void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  return solve_qp_elastic_impl(d, Q, q, G, h, penalty, solver_tol, x, t, s1, s2, z1, z2, converged, iters, cfg, ws,
+                               ws_bytes, stream, false);
+}
+
+int qpb_tune_solve_qp_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G,
+                              const double* h, const double* penalty, double solver_tol, double* x, double* t,
+                              double* s1, double* s2, double* z1, double* z2, int32_t* converged, int32_t* iters,
+                              const qpb_config* cfg, void* ws, size_t ws_bytes, qpb_stream_t stream) {
+  return solve_qp_elastic_impl(d, Q, q, G, h, penalty, solver_tol, x, t, s1, s2, z1, z2, converged, iters, cfg, ws,
+                               ws_bytes, stream, true);
 }
 
 int qpb_initialize_elastic(const qpb_dims* d, const double* Q, const double* q, const double* G, const double* h,

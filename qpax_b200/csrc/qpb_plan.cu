@@ -24,6 +24,7 @@ struct PlanBin {
   size_t ws_off;     // bin's slice of the caller's workspace
   double work;       // estimated cost (for launch order)
   int n_max, m_max, p_max;
+  int key;           // kernel-variant key (bin_key)
 };
 
 }  // namespace qpb
@@ -63,6 +64,16 @@ static int bin_key(const qpb_dims& d, const qpb_config& c) {
   if (!mixed && np && (c.team_threads == 0 || c.team_threads == 32)) return np;  // 8, 16, 32
   const int kc = chunks_for(d.n > d.m ? d.n : d.m);
   return 1000 + kc;  // team kernel, KC register chunks
+}
+
+// Workspace slices of the bins, in launch order.
+static void layout_workspace(qpb_plan* pl) {
+  size_t ws = 0;
+  for (PlanBin& b : pl->bins) {
+    b.ws_off = ws;
+    ws += (b.launch.ws_bytes + 255) & ~size_t(255);
+  }
+  pl->ws_bytes = ws ? ws : 256;
 }
 
 }  // namespace qpb
@@ -139,7 +150,10 @@ int qpb_plan_create(qpb_plan** out, int32_t batch, const int32_t* shapes, const 
     std::stable_sort(list.begin() + b.list_off, list.end(),
                      [&](int32_t x, int32_t y) { return inst_work(x) > inst_work(y); });
     const qpb_dims dm{b.count, b.n_max, b.m_max, b.p_max};
-    // size the launch for the largest member; the backward op needs the same arena
+    b.key = key;
+    // size the launch for the largest member; the backward op needs the same
+    // arena.  A launch shape tuned earlier on this device for a bin with the
+    // same largest (n, m, p) is reused (make_plan looks it up).
     int st = make_plan(kOpSolve, dm, c, &b.launch);
     if (st) {
       free_plan(pl);
@@ -150,13 +164,7 @@ int qpb_plan_create(qpb_plan** out, int32_t batch, const int32_t* shapes, const 
     pl->bins.push_back(b);
   }
   std::sort(pl->bins.begin(), pl->bins.end(), [](const PlanBin& x, const PlanBin& y) { return x.work > y.work; });
-  // recompute workspace slices in launch order
-  ws = 0;
-  for (PlanBin& b : pl->bins) {
-    b.ws_off = ws;
-    ws += (b.launch.ws_bytes + 255) & ~size_t(255);
-  }
-  pl->ws_bytes = ws ? ws : 256;
+  layout_workspace(pl);
   if (batch > 0) {
     if (cudaMalloc(&pl->d_shapes, sizeof(int32_t) * pl->shapes.size()) != cudaSuccess ||
         cudaMalloc(&pl->d_offs, sizeof(int64_t) * pl->offs.size()) != cudaSuccess ||
@@ -306,6 +314,86 @@ int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const 
   P.conv = converged;
   P.iters = iters;
   return launch_packed(plan, P, workspace, workspace_bytes, stream);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+size_t qpb_plan_tune_workspace_size(const qpb_plan* plan) {
+  if (!plan) return 0;
+  size_t need = plan->ws_bytes;
+  for (const PlanBin& b : plan->bins) {
+    const qpb_dims d{b.count, b.n_max, b.m_max, b.p_max};
+    const size_t w = tune_workspace(kOpSolve, d, plan->cfg);
+    if (w > need) need = w;
+  }
+  return need;
+}
+
+int qpb_plan_tune(qpb_plan* plan, const double* Q, const double* q, const double* A, const double* b,
+                  const double* G, const double* h, double solver_tol, double* x, double* s, double* z, double* y,
+                  int32_t* converged, int32_t* iters, void* workspace, size_t workspace_bytes,
+                  qpb_stream_t stream) {
+  if (!plan) return QPB_ERR_INVALID_ARGUMENT;
+  const int64_t* t = plan->totals;
+  if (!ok_ptr(Q, t[0]) || !ok_ptr(q, t[1]) || !ok_ptr(A, t[2]) || !ok_ptr(b, t[3]) || !ok_ptr(G, t[4]) ||
+      !ok_ptr(h, t[5]) || !ok_ptr(x, t[1]) || !ok_ptr(s, t[5]) || !ok_ptr(z, t[5]) || !ok_ptr(y, t[3]) ||
+      (plan->batch && (!converged || !iters)))
+    return QPB_ERR_INVALID_ARGUMENT;
+  if (plan->batch == 0) return QPB_OK;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != plan->device) return QPB_ERR_INVALID_ARGUMENT;
+  if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255)) return QPB_ERR_WORKSPACE;
+  if (plan->cfg.team_threads != 0) {  // the caller fixed the launch shape
+    if (workspace_bytes < plan->ws_bytes) return QPB_ERR_WORKSPACE;
+    return qpb_solve_qp_packed(plan, Q, q, A, b, G, h, solver_tol, x, s, z, y, converged, iters, workspace,
+                               workspace_bytes, stream);
+  }
+  Params P{};
+  P.op = kOpSolve;
+  P.tol = solver_tol;
+  P.Q = Q; P.q = q; P.A = A; P.b = b; P.G = G; P.h = h;
+  P.out[0] = x; P.out[1] = s; P.out[2] = z; P.out[3] = y;
+  P.conv = converged;
+  P.iters = iters;
+  P.shapes = plan->d_shapes;
+  P.offs = plan->d_offs;
+  P.mixed = plan->cfg.precision == QPB_PRECISION_MIXED;
+  P.pivot_max = plan->cfg.pivot_max;
+  P.max_sweeps = plan->cfg.max_sweeps;
+  for (PlanBin& bn : plan->bins) {
+    const qpb_dims d{bn.count, bn.n_max, bn.m_max, bn.p_max};
+    P.list = plan->d_list + bn.list_off;  // the bin's instances, heaviest first
+    LaunchChoice best{};
+    const int status = tune_pick(P, kOpSolve, d, plan->cfg, workspace, workspace_bytes, stream, &best);
+    if (status != QPB_OK) return status;
+    Plan full;  // the chosen shape, sized for the whole bin
+    if (make_plan(kOpSolve, d, plan->cfg, &full, &best) == QPB_OK) {
+      bn.launch = full;
+      tune_record(kOpSolve, d, plan->cfg, best);
+    }
+  }
+  layout_workspace(plan);
+  if (workspace_bytes < plan->ws_bytes) return QPB_ERR_WORKSPACE;
+  // outputs for the whole batch with the tuned plan
+  return qpb_solve_qp_packed(plan, Q, q, A, b, G, h, solver_tol, x, s, z, y, converged, iters, workspace,
+                             workspace_bytes, stream);
+}
+
+int32_t qpb_plan_bin_info(const qpb_plan* plan, int32_t bin, int32_t info[8]) {
+  if (!plan || !info || bin < 0 || bin >= (int32_t)plan->bins.size()) return QPB_ERR_INVALID_ARGUMENT;
+  const PlanBin& b = plan->bins[bin];
+  const int sms = device_sms();
+  info[0] = b.count;
+  info[1] = b.n_max;
+  info[2] = b.m_max;
+  info[3] = b.p_max;
+  info[4] = b.launch.threads / b.launch.teams;  // threads per instance team
+  info[5] = b.launch.in_smem ? 1 : 2;
+  info[6] = b.launch.gstage_rows;
+  info[7] = sms > 0 ? (b.launch.grid + sms - 1) / sms : 0;  // resident CTAs per SM
+  return QPB_OK;
 }
 
 }  // extern "C"

@@ -81,7 +81,17 @@ struct WarpAddr {
   QPB_DEV double* F() const { return Y() + (MP > 8 ? MP : 8) * (NP + 1); }
 };
 
-template <int NP, int MP>
+// Code-shape options of the warp kernel (bit set).
+enum WarpOpt : unsigned {
+  kWoFReg = 1,    // factor the m x m Schur complement F in registers
+  kWoFuseY = 2,   // form Y = L^-1 A' inside the LDL^T loop
+  kWoOneFma = 4,  // LDL^T update as one FMA per element (l = S[k][j] / d_k)
+  kWoXsm = 8,     // residuals: x broadcast through shared memory for Q x
+  kWoHpre = 16,   // H formation k-loop unrolled by two
+  kWoVecLds = 32  // LDL^T: pivot row read as 16-byte pairs
+};
+
+template <int NP, int MP, unsigned kOpt = 0>
 struct WarpQP {
   static_assert(NP == 8 || NP == 16 || NP == 32, "NP");
   static constexpr int kYld = NP + 1;  // row stride of Y
@@ -262,6 +272,7 @@ struct WarpQP {
 #pragma unroll
     for (int tj = 0; tj <= TI; ++tj) acc[tj][0] = acc[tj][1] = 0.0;
     const int sw = gswz(t);  // = gswz(4 kb + t)
+#pragma unroll((kOpt & kWoHpre) ? 2 : 1)
     for (int kb = 0; kb < kblocks; ++kb) {
       const int k = 4 * kb + t;
       const bool in = k < p;
@@ -329,9 +340,21 @@ struct WarpQP {
     // LDL^T: step k broadcasts row k of the Schur complement (= column k)
     int bad = 0;
     double* cb = a.cb();
+    double yc[MP];
+    double* yb = a.Y();  // fused Y: lane k's column of Y (free until Y is stored)
+    if constexpr ((kOpt & kWoFuseY) != 0) {
+#pragma unroll
+      for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
+    }
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       if (lane < NP) cb[lane] = hc[k];
+      if constexpr ((kOpt & kWoFuseY) != 0) {
+        if (lane == k) {
+#pragma unroll
+          for (int i = 0; i < MP; ++i) yb[i] = yc[i];
+        }
+      }
       __syncwarp();
       const double dk = cb[k];
       const double rk = 1.0 / dk;
@@ -342,22 +365,52 @@ struct WarpQP {
       // row-held and column-held copies of L agree exactly.
       const double hk = hc[k];
       if (lane > k) {
+        if constexpr ((kOpt & kWoOneFma) != 0) {
+          const double l = hk * rk;
+          if constexpr ((kOpt & kWoVecLds) != 0) {
+            if ((k + 1) & 1) hc[k + 1] = fma(-cb[k + 1], l, hc[k + 1]);
 #pragma unroll
-        for (int i = k + 1; i < NP; ++i) hc[i] = fma(-(cb[i] * hk), rk, hc[i]);
+            for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
+              const double2 c2 = *reinterpret_cast<const double2*>(cb + i2);
+              hc[i2] = fma(-c2.x, l, hc[i2]);
+              hc[i2 + 1] = fma(-c2.y, l, hc[i2 + 1]);
+            }
+          } else {
+#pragma unroll
+            for (int i = k + 1; i < NP; ++i) hc[i] = fma(-cb[i], l, hc[i]);
+          }
+        } else if constexpr ((kOpt & kWoVecLds) != 0) {
+          if ((k + 1) & 1) hc[k + 1] = fma(-(cb[k + 1] * hk), rk, hc[k + 1]);
+#pragma unroll
+          for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
+            const double2 c2 = *reinterpret_cast<const double2*>(cb + i2);
+            hc[i2] = fma(-(c2.x * hk), rk, hc[i2]);
+            hc[i2 + 1] = fma(-(c2.y * hk), rk, hc[i2 + 1]);
+          }
+        } else {
+#pragma unroll
+          for (int i = k + 1; i < NP; ++i) hc[i] = fma(-(cb[i] * hk), rk, hc[i]);
+        }
+        if constexpr ((kOpt & kWoFuseY) != 0) {
+          const double l = hk * rk;  // = L[lane][k], as the separate Y loop forms it
+#pragma unroll
+          for (int i = 0; i < MP; ++i) yc[i] = fma(-l, yb[i], yc[i]);
+        }
       }
       __syncwarp();
     }
     if (lane < NP) a.dvi()[lane] = dinv;
     __syncwarp();
-    // Y = L^-1 A'   (unit L; L[j][k] = hc[k] * dinv_k for lane j > k)
-    double yc[MP];
+    if constexpr ((kOpt & kWoFuseY) == 0) {
+      // Y = L^-1 A'   (unit L; L[j][k] = hc[k] * dinv_k for lane j > k)
 #pragma unroll
-    for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
+      for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
 #pragma unroll
-    for (int k = 0; k < NP - 1; ++k) {
-      const double l = (lane > k && lane < NP) ? hc[k] * a.dvi()[k] : 0.0;
+      for (int k = 0; k < NP - 1; ++k) {
+        const double l = (lane > k && lane < NP) ? hc[k] * a.dvi()[k] : 0.0;
 #pragma unroll
-      for (int i = 0; i < MP; ++i) yc[i] = fma(-l, __shfl_sync(kFull, yc[i], k), yc[i]);
+        for (int i = 0; i < MP; ++i) yc[i] = fma(-l, __shfl_sync(kFull, yc[i], k), yc[i]);
+      }
     }
     if (lane < NP) {
 #pragma unroll
@@ -380,17 +433,49 @@ struct WarpQP {
       Fm[e] = v;
     }
     __syncwarp();
-    // LDL^T of F in the same in-place layout as H: lane c owns column c
-    for (int k = 0; k < MP; ++k) {
-      const double dk = Fm[k * MP + k];
-      const double rk = 1.0 / dk;
-      if (k < m) bad |= !(dk > 0.0) || !isfinite(dk);
-      if (lane == k) fdinv = rk;
-      if (lane > k && lane < MP) {
-        const double f = Fm[k * MP + lane] * rk;
-        for (int i = k + 1; i < MP; ++i) Fm[i * MP + lane] = fma(-Fm[i * MP + k], f, Fm[i * MP + lane]);
+    if constexpr ((kOpt & kWoFReg) != 0) {
+      // LDL^T of F in registers, lane c owning column c; step k broadcasts
+      // column k (the operands and order of the shared-memory form below)
+      double fc[MP];
+#pragma unroll
+      for (int i = 0; i < MP; ++i) fc[i] = (lane < MP) ? Fm[i * MP + lane] : 0.0;
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < MP; ++k) {
+        if (lane == k) {
+#pragma unroll
+          for (int i = 0; i < MP; ++i) cb[i] = fc[i];
+        }
+        __syncwarp();
+        const double dk = cb[k];
+        const double rk = 1.0 / dk;
+        if (k < m) bad |= !(dk > 0.0) || !isfinite(dk);
+        if (lane == k) fdinv = rk;
+        if (lane > k && lane < MP) {
+          const double f = fc[k] * rk;
+#pragma unroll
+          for (int i = k + 1; i < MP; ++i) fc[i] = fma(-cb[i], f, fc[i]);
+        }
+        __syncwarp();
+      }
+      if (lane < MP) {
+#pragma unroll
+        for (int i = 0; i < MP; ++i) Fm[i * MP + lane] = fc[i];
       }
       __syncwarp();
+    } else {
+      // LDL^T of F in the same in-place layout as H: lane c owns column c
+      for (int k = 0; k < MP; ++k) {
+        const double dk = Fm[k * MP + k];
+        const double rk = 1.0 / dk;
+        if (k < m) bad |= !(dk > 0.0) || !isfinite(dk);
+        if (lane == k) fdinv = rk;
+        if (lane > k && lane < MP) {
+          const double f = Fm[k * MP + lane] * rk;
+          for (int i = k + 1; i < MP; ++i) Fm[i * MP + lane] = fma(-Fm[i * MP + k], f, Fm[i * MP + lane]);
+        }
+        __syncwarp();
+      }
     }
     if (bad) st_flags |= kFlagBreakdown64;
   }
@@ -512,7 +597,15 @@ struct WarpQP {
   // qpax/pdip.py:93-100, pdip_relaxed.py:16-23.
   QPB_DEV double residuals(double kappa, double& v1, double& v4) {
     double qx = 0.0;
-    {
+    if constexpr ((kOpt & kWoXsm) != 0) {
+      if (lane < NP) a.xs()[lane] = x;
+      __syncwarp();
+      double qv[NP];
+      load_q(qv);
+      const double* xsv = a.xs();
+#pragma unroll
+      for (int i = 0; i < NP; ++i) qx = fma(qv[i], xsv[i], qx);
+    } else {
       double qv[NP];
       load_q(qv);
 #pragma unroll

@@ -59,9 +59,9 @@ def _arr6(ts):
     return (ctypes.c_void_p * 6)(*[ptr(t) for t in ts])
 
 
-def _run(name, op, bt: ElasticBatch, cfg, mid):
+def _run(name, op, bt: ElasticBatch, cfg, mid, tune=False):
     dims = bt.dims()
-    ws = _lib.workspace(op, dims, cfg, bt.dev)
+    ws = _lib.workspace(op, dims, cfg, bt.dev, tune)
     wp, wb = _lib.aligned(ws)
     _lib.call(name, ctypes.byref(dims), *bt.ptrs(), *mid, ctypes.byref(cfg), wp, wb, _lib.stream_handle())
 
@@ -75,6 +75,19 @@ def solve_qp_elastic(Q, q, G, h, penalty, solver_tol: float = 1e-3, *, precision
     conv, iters = bt.new(bt.B, dtype=torch.int32), bt.new(bt.B, dtype=torch.int32)
     _run("qpb_solve_qp_elastic", "elastic_solve", bt, cfg,
          [ctypes.c_double(solver_tol)] + [ptr(t) for t in it] + [ptr(conv), ptr(iters)])
+    return bt.out(*it, conv, iters)
+
+
+def tune_solve_qp_elastic(Q, q, G, h, penalty, solver_tol: float = 1e-3, *, precision=None):
+    """solve_qp_elastic with the launch shape autotuned for these dims on this
+    device (qpb_tune_solve_qp_elastic); later elastic calls with these dims
+    use the recorded shape.  Returns what solve_qp_elastic returns."""
+    bt = ElasticBatch(Q, q, G, h, penalty)
+    cfg = _config(dict(precision=precision))
+    it = bt.iterate()
+    conv, iters = bt.new(bt.B, dtype=torch.int32), bt.new(bt.B, dtype=torch.int32)
+    _run("qpb_tune_solve_qp_elastic", "elastic_solve", bt, cfg,
+         [ctypes.c_double(solver_tol)] + [ptr(t) for t in it] + [ptr(conv), ptr(iters)], tune=True)
     return bt.out(*it, conv, iters)
 
 

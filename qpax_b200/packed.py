@@ -29,6 +29,10 @@ _SIGS = {
     "qpb_plan_workspace_size": ([ctypes.c_void_p], ctypes.c_size_t),
     "qpb_plan_num_bins": ([ctypes.c_void_p], ctypes.c_int32),
     "qpb_plan_totals": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "qpb_plan_tune_workspace_size": ([ctypes.c_void_p], ctypes.c_size_t),
+    "qpb_plan_tune": ([ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_double] + [ctypes.c_void_p] * 6 +
+                      [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p], ctypes.c_int),
+    "qpb_plan_bin_info": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p], ctypes.c_int32),
     "qpb_solve_qp_packed": ([ctypes.c_void_p] + [ctypes.c_void_p] * 6 + [ctypes.c_double] + [ctypes.c_void_p] * 6 +
                             [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p], ctypes.c_int),
     "qpb_solve_qp_primal_bwd_packed": ([ctypes.c_void_p] + [ctypes.c_void_p] * 11 + [ctypes.c_double] * 2 +
@@ -114,6 +118,36 @@ class PackedPlan:
                   ctypes.c_double(solver_tol), *[_lib.ptr(t) for t in (x, s, z, y, conv, iters)], wp, wb,
                   _lib.stream_handle())
         return x, s, z, y, conv, iters
+
+    def tune(self, Q, q, A, b, G, h, solver_tol: float = 1e-3):
+        """qpb_plan_tune: time the launch shapes the kernels support for each
+        size bin on this batch (forward solve on each bin's heaviest
+        instances), keep the fastest per bin and record it for this device.
+        Returns the packed solve outputs, like solve()."""
+        tw = int(self.lib.qpb_plan_tune_workspace_size(self.handle))
+        ws = torch.empty(tw + 256, dtype=torch.uint8, device=self.dev)
+        wp, wb = _lib.aligned(ws)
+        x, s, z, y = self.new(1), self.new(5), self.new(5), self.new(3)
+        conv = torch.empty(self.batch, dtype=torch.int32, device=self.dev)
+        iters = torch.empty(self.batch, dtype=torch.int32, device=self.dev)
+        _lib.call("qpb_plan_tune", self.handle, *[_lib.ptr(t) for t in (Q, q, A, b, G, h)],
+                  ctypes.c_double(solver_tol), *[_lib.ptr(t) for t in (x, s, z, y, conv, iters)], wp, wb,
+                  _lib.stream_handle())
+        nbytes = int(self.lib.qpb_plan_workspace_size(self.handle))
+        if nbytes + 256 > self.workspace.numel():
+            self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.dev)
+        return x, s, z, y, conv, iters
+
+    def bin_info(self):
+        """Per bin (launch order): dict of its instances, largest shape and launch shape."""
+        out = []
+        for k in range(self.num_bins):
+            info = (ctypes.c_int32 * 8)()
+            self.lib.qpb_plan_bin_info(self.handle, k, ctypes.addressof(info))
+            v = list(info)
+            out.append(dict(instances=v[0], n_max=v[1], m_max=v[2], p_max=v[3], team_threads=v[4],
+                            arena="shared" if v[5] == 1 else "global", g_chunk_rows=v[6], ctas_per_sm=v[7]))
+        return out
 
     def primal_bwd(self, Q, q, A, b, G, h, x, s, z, y, dl_dx, solver_tol: float = 1e-5,
                    target_kappa: float = 1e-3, relax_out=None):

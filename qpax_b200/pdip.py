@@ -72,9 +72,9 @@ class StdBatch:
         return tuple(ts) if self.batched else tuple(t[0] for t in ts)
 
 
-def _run(name: str, op: str, bt: StdBatch, cfg: _lib.Config, mid: list, tail: list) -> None:
+def _run(name: str, op: str, bt: StdBatch, cfg: _lib.Config, mid: list, tail: list, tune: bool = False) -> None:
     dims = bt.dims()
-    ws = _lib.workspace(op, dims, cfg, bt.dev)
+    ws = _lib.workspace(op, dims, cfg, bt.dev, tune)
     wp, wb = _lib.aligned(ws)
     _lib.call(name, ctypes.byref(dims), *bt.ptrs(), *mid, *tail, ctypes.byref(cfg), wp, wb, _lib.stream_handle())
 
@@ -113,3 +113,17 @@ def relax_qp(Q, q, A, b, G, h, x, s, z, y, solver_tol: float = 1e-5, target_kapp
          [ptr(t) for t in its] + [ctypes.c_double(solver_tol), ctypes.c_double(target_kappa)],
          [ptr(xr), ptr(sr), ptr(zr), ptr(yr), ptr(conv), ptr(iters)])
     return bt.out(xr, sr, zr, yr, conv, iters)
+
+
+def tune_solve_qp(Q, q, A, b, G, h, solver_tol: float = 1e-3, *, precision=None):
+    """solve_qp with the launch shape autotuned for this (n, m, p) on this
+    device (qpb_tune_solve_qp): the candidates are timed on the batch, the
+    fastest is recorded, and later calls with these dims use it.  Returns what
+    solve_qp returns."""
+    bt = StdBatch(Q, q, A, b, G, h)
+    cfg = _config(dict(precision=precision))
+    x, s, z, y = bt.new(bt.B, bt.n), bt.new(bt.B, bt.p), bt.new(bt.B, bt.p), bt.new(bt.B, bt.m)
+    conv, iters = bt.new(bt.B, dtype=torch.int32), bt.new(bt.B, dtype=torch.int32)
+    _run("qpb_tune_solve_qp", "solve", bt, cfg, [ctypes.c_double(solver_tol)],
+         [ptr(x), ptr(s), ptr(z), ptr(y), ptr(conv), ptr(iters)], tune=True)
+    return bt.out(x, s, z, y, conv, iters)
