@@ -351,6 +351,10 @@ class UniformArm:
         self.gx = torch.empty(B, n, dtype=torch.float64, device=dev)
         self.grads = None
         self.launches = 2
+        if opts.get("tune"):  # launch shape timed and recorded for these dims (untimed setup)
+            import qpax_b200 as qb
+
+            qb.tune_solve_qp(*self.dev_in, spec.tol, precision=opts.get("precision"))
 
     def fwd(self):
         from qpax_b200.pdip import _run
@@ -376,10 +380,33 @@ class UniformArm:
 
         dl = self.gx.cpu().numpy()
         return parity.standard(data, self.spec.tol, KAPPA, dl, self.x.cpu().numpy(), self.conv.cpu().numpy(),
-                               self.iters.cpu().numpy(), [g.cpu().numpy() for g in self.grads])[0]
+                               self.iters.cpu().numpy(), [g.cpu().numpy() for g in self.grads], perturb=2)[0]
 
     def kernel_name(self, which):
         return "qpb_solve_qp (forward)" if which == "forward" else "qpb_solve_qp_primal_bwd (backward)"
+
+    def precision_stats(self):
+        """Per-instance FP32 / FP64 factorisations and FP64 refinement sweeps of
+        one forward solve and one relaxation (the optional stats output of the
+        C ABI), as means over the batch; untimed."""
+        import torch
+
+        import qpax_b200 as qb
+
+        B = self.spec.batch
+        out = {}
+        st = torch.zeros(B, 4, dtype=torch.int32, device=self.x.device)
+        x, s, z, y, _, _ = qb.solve_qp(*self.dev_in, self.spec.tol, precision=self.opts.get("precision"), stats=st)
+        out["forward"] = st.double().mean(0).tolist()
+        fwd_flags = st[:, 3].cpu().numpy()
+        st.zero_()
+        qb.relax_qp(*self.dev_in, x, s, z, y, self.spec.tol, KAPPA, precision=self.opts.get("precision"), stats=st)
+        out["relaxation"] = st.double().mean(0).tolist()
+        res = {k: {"fp32_factorisations": v[0], "fp64_factorisations": v[1], "refinement_sweeps": v[2]}
+               for k, v in out.items()}
+        res["forward"]["share_with_fp32_factor_rejected"] = float(((fwd_flags & 1) != 0).mean())
+        res["note"] = "means per instance; FP64 refactor when the FP32 pivot ratio exceeds pivot_max or refinement stalls"
+        return res
 
 
 class ElasticArm:
@@ -398,6 +425,11 @@ class ElasticArm:
         self.out = None
         self.grads = None
         self.launches = 2
+        self.opts = {k: v for k, v in opts.items() if k != "tune"}
+        if opts.get("tune"):
+            import qpax_b200 as qb
+
+            qb.tune_solve_qp_elastic(*self.dev_in, self.pen, spec.tol, precision=opts.get("precision"))
 
     def fwd(self):
         import qpax_b200 as qb
@@ -424,7 +456,8 @@ class ElasticArm:
         from oracle import parity
 
         return parity.elastic(tuple(data), 1e3, self.spec.tol, KAPPA, self.gx.cpu().numpy(),
-                              [t.cpu().numpy() for t in self.out], [g.cpu().numpy() for g in self.grads])[0]
+                              [t.cpu().numpy() for t in self.out], [g.cpu().numpy() for g in self.grads], perturb=2,
+                              g_bar=1e-4)[0]
 
     def kernel_name(self, which):
         return ("qpb_solve_qp_elastic (forward)" if which == "forward"
@@ -446,6 +479,8 @@ class UnevenArm:
         self.plan = PackedPlan(list(zip(n, m, p)), precision=opts.get("precision") or "auto",
                                team_threads=opts.get("team_threads") or 0)
         self.ins = [pack(v, dev) for v in data]
+        if opts.get("tune"):
+            self.plan.tune(*self.ins, spec.tol)
         B = spec.batch
         self.rconv = torch.empty(B, dtype=torch.int32, device=dev)
         self.riters = torch.empty(B, dtype=torch.int32, device=dev)
@@ -500,7 +535,7 @@ class UnevenArm:
         sub = [v[:k] for v in data]
         fig = parity.standard(sub, self.spec.tol, KAPPA, cut(self.gx, 1), cut(self.out[0], 1),
                               self.out[4][:k].cpu().numpy(), self.out[5][:k].cpu().numpy(),
-                              [cut(self.grads[f], f) for f in range(6)])[0]
+                              [cut(self.grads[f], f) for f in range(6)], perturb=2)[0]
         fig["sample"] = f"the first {k} instances of the batch"
         return fig
 
@@ -514,8 +549,8 @@ class UnevenArm:
 ARMS = {"uniform": UniformArm, "elastic": ElasticArm, "uneven": UnevenArm}
 
 
-def variants_for(spec: Spec):
-    v = {"auto": dict(precision="auto")}
+def variants_for(spec: Spec, tune=True):
+    v = {"auto": dict(precision="auto", tune=tune)}
     if spec.kind != "elastic":
         v["fp64_cta"] = dict(precision="fp64", team_threads=128)  # plain FP64, one QP per CTA
     v["mixed"] = dict(precision="mixed")                          # FP32 factor + FP64 refinement
@@ -567,7 +602,7 @@ def run_ours(args, spec: Spec, world, rank, local):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     results = {}
-    variants = variants_for(spec)
+    variants = variants_for(spec, tune=not args.no_tune)
     if args.only_default:
         variants = {"auto": variants["auto"]}
     arm_main = None
@@ -577,8 +612,9 @@ def run_ours(args, spec: Spec, world, rank, local):
         tot, fwd_ms, bwd_ms = time_arm(args, arm, stream, flush, world, args.steps, sampler)
         conv, iters, riters = arm.counts()
         par = arm.parity(data) if (rank == 0 and not args.no_parity) else None
+        pstats = arm.precision_stats() if (prec == "mixed" and hasattr(arm, "precision_stats")) else None
         results[prec] = dict(total_ms=tot, fwd_ms=fwd_ms, bwd_ms=bwd_ms, conv=conv, iters=iters, riters=riters,
-                             clocks=sampler.summary() if sampler else None, parity=par)
+                             clocks=sampler.summary() if sampler else None, parity=par, pstats=pstats)
         if prec == "auto":
             arm_main = arm
         else:
@@ -621,6 +657,7 @@ def run_ours(args, spec: Spec, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_for(spec, world, extra={
             "precision": prec_desc, "parallelism": f"batch split x{world}",
+            "launch_shapes": "heuristic" if args.no_tune else "autotuned per size bin at setup (untimed)",
             "l2": "flushed between steps (256 MB write), outside the per-step events"}),
         "roofline": roof, "gpu_launches": arm_main.launches * args.steps,
         "iterations": {"forward_mean": float(main_r["iters"].mean()), "relax_mean": float(main_r["riters"].mean()),
@@ -635,12 +672,17 @@ def run_ours(args, spec: Spec, world, rank, local):
         plain = "fp64_cta" if "fp64_cta" in v else "auto"
         if "mixed" in v:
             line["mixed_over_plain_fp64"] = v["mixed"] / v[plain]
+            if results["mixed"]["pstats"]:
+                line["variants"][VARIANT_NAMES["mixed"]]["precision_stats"] = results["mixed"]["pstats"]
         line["default_over_plain_fp64"] = v["auto"] / v[plain]
     if rank == 0 and not args.no_parity:
         line["parity"] = {VARIANT_NAMES[k]: r["parity"] for k, r in results.items()}
         line["parity"]["against"] = ("the FP64 oracle (C restatement of qpax) on the same inputs and the same dl/dx, "
                                      "computed after the timed steps; errors relative per instance, "
-                                     "||gpu - ref||_inf / max(1, ||ref||_inf); objective 1/2 x'Qx + q'x")
+                                     "||gpu - ref||_inf / max(1, ||ref||_inf); objective 1/2 x'Qx + q'x; "
+                                     "'reproducible' = the oracle gives the same flag and iteration count (and a "
+                                     "gradient within a tenth of the 1e-5 bar) on two runs with inputs perturbed by "
+                                     "1e-15 relative")
     if not args.no_e2e:  # every rank takes part (barriers, max over ranks)
         e2e = run_e2e(args, spec, data, dev, arm_main, world)
         if rank == 0:
@@ -666,7 +708,7 @@ def run_configs(args, world, rank, dev, stream, flush):
     for key in ("nnls", "small", "uneven", "elastic"):
         spec = WORKLOADS[key]
         data = make_data(spec)
-        arm = ARMS[spec.kind](spec, data, dev, dict(precision="auto"))
+        arm = ARMS[spec.kind](spec, data, dev, dict(precision="auto", tune=not args.no_tune))
         steps = args.config_steps
         tot, fwd_ms, bwd_ms = time_arm(args, arm, stream, flush, world, steps)
         conv, iters, riters = arm.counts()
@@ -815,6 +857,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity figures")
+    ap.add_argument("--no-tune", action="store_true", help="heuristic launch shapes (no autotuning at setup)")
     ap.add_argument("--no-configs", action="store_true",
                     help="dense workload: skip the other four configurations' block")
     ap.add_argument("--config-steps", type=int, default=5, help="timed steps of each configuration in the block")

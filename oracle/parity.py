@@ -5,6 +5,18 @@ timed region): the oracle is the checker here, never the thing measured.
 
 Per-instance relative error of an array: ||gpu - ref||_inf / max(1, ||ref||_inf).
 Objective: 1/2 x'Qx + q'x (elastic: plus penalty * sum(t)), relative the same way.
+
+Reproducibility of the reference.  On ill-conditioned instances qpax's own
+FP64 method decides its outcome by rounding: its residual reaches ~tol late
+in the loop, where the reduced KKT matrix has cond ~1e14 and beyond, and
+whether one more step lands below tol is a coin flip.  Run on inputs
+perturbed at the rounding level (relative 1e-15, symmetric in Q), the oracle
+itself then changes its converged flag or iteration count, and (in qpax's
+elastic relaxation, which runs to its iteration cap) its output by up to
+1e-2.  With `perturb=K`, the figures include that spread over K perturbed
+runs, and the mismatch counts restricted to the instances whose reference
+outcome is reproducible: same flag and iteration count in every perturbed
+run, and for gradients a spread below a tenth of the gradient bar.
 """
 
 from __future__ import annotations
@@ -46,7 +58,65 @@ def _finite_max(v):
     return float(v.max()) if v.size else 0.0
 
 
-def standard(data, tol, kappa, dl, gpu_x, gpu_conv, gpu_iters, gpu_grads, ref=None):
+def perturb_inputs(data, eps, seed):
+    """Copies of (Q, q, A, b, G, h) or (Q, q, G, h) with every entry scaled by
+    (1 + eps N(0, 1)); Q's perturbation is symmetric."""
+    rng = np.random.default_rng(seed)
+
+    def one(a, sym=False):
+        a = np.asarray(a, np.float64)
+        e = rng.standard_normal(a.shape)
+        if sym:
+            e = 0.5 * (e + np.swapaxes(e, -1, -2))
+        return a * (1.0 + eps * e)
+
+    out = []
+    for k, v in enumerate(data):
+        if isinstance(v, (list, tuple)):
+            out.append([one(a, sym=(k == 0)) for a in v])
+        else:
+            out.append(one(v, sym=(k == 0)))
+    return out
+
+
+def _spread(ref, runs, B, key):
+    sp = np.zeros(B)
+    for r in runs:
+        if key == "grads":
+            for g, go in zip(r["grads"], ref["grads"]):
+                sp = np.maximum(sp, rel_errors(g, go, B))
+        else:
+            sp = np.maximum(sp, rel_errors(r[key], ref[key], B))
+    return sp
+
+
+def _figures(B, gpu_conv, gpu_iters, ex, eo, eg, ref, g_bar):
+    gpu_conv, gpu_iters = np.asarray(gpu_conv), np.asarray(gpu_iters)
+    both = (gpu_conv == 1) & (ref["conv"] == 1)
+    fig = {
+        "instances": int(B),
+        "compared": int(both.sum()),
+        "max_err_x": _finite_max(ex[both]),
+        "max_err_obj": _finite_max(eo[both]),
+        "max_err_grad": _finite_max(eg[both]),
+        "conv_mismatch": int((gpu_conv != ref["conv"]).sum()),
+        "iters_mismatch": int((gpu_iters != ref["iters"]).sum()),
+        "reference_not_converged": int((ref["conv"] != 1).sum()),
+    }
+    if "stable" in ref:
+        st, gst = ref["stable"], ref["grad_stable"]
+        fig.update({
+            "reference_outcome_not_reproducible": int((~st).sum()),
+            "conv_mismatch_reproducible": int(((gpu_conv != ref["conv"]) & st).sum()),
+            "iters_mismatch_reproducible": int(((gpu_iters != ref["iters"]) & st).sum()),
+            "reference_grad_not_reproducible": int((both & ~gst).sum()),
+            "max_err_grad_reproducible": _finite_max(eg[both & gst]),
+            "reference_perturbed_runs": int(ref["perturbed_runs"]),
+        })
+    return fig
+
+
+def standard(data, tol, kappa, dl, gpu_x, gpu_conv, gpu_iters, gpu_grads, ref=None, perturb=0, g_bar=1e-5):
     """Parity of a solve_qp_primal forward + backward against the oracle.
 
     data: (Q, q, A, b, G, h), uniform arrays or ragged lists; dl: the incoming
@@ -55,41 +125,46 @@ def standard(data, tol, kappa, dl, gpu_x, gpu_conv, gpu_iters, gpu_grads, ref=No
     """
     Q, q, A, b, G, h = data
     B = len(q) if isinstance(q, (list, tuple)) else np.asarray(q).shape[0]
+
+    def run(d):
+        x, grads, conv, iters = oracle.solve_qp_primal_vjp(*d, dl, solver_tol=tol, target_kappa=kappa)
+        return dict(x=x, grads=grads, conv=np.asarray(conv), iters=np.asarray(iters))
+
     if ref is None:
-        x_o, grads_o, conv_o, iters_o = oracle.solve_qp_primal_vjp(*data, dl, solver_tol=tol, target_kappa=kappa)
-        ref = dict(x=x_o, grads=grads_o, conv=np.asarray(conv_o), iters=np.asarray(iters_o))
-    both = (np.asarray(gpu_conv) == 1) & (ref["conv"] == 1)
+        ref = run(data)
+    if perturb and "stable" not in ref:
+        runs = [run(perturb_inputs(data, 1e-15, 1000 + k)) for k in range(perturb)]
+        ref["stable"] = np.all([(r["conv"] == ref["conv"]) & (r["iters"] == ref["iters"]) for r in runs], axis=0)
+        ref["grad_stable"] = ref["stable"] & (_spread(ref, runs, B, "grads") <= 0.1 * g_bar)
+        ref["perturbed_runs"] = perturb
     ex = rel_errors(gpu_x, ref["x"], B)
     fo, fg = objective(Q, q, ref["x"], B), objective(Q, q, gpu_x, B)
     eo = np.abs(fg - fo) / np.maximum(1.0, np.abs(fo))
     eg = np.zeros(B)
     for g, go in zip(gpu_grads, ref["grads"]):
         eg = np.maximum(eg, rel_errors(g, go, B))
-    fig = {
-        "instances": int(B),
-        "compared": int(both.sum()),
-        "max_err_x": _finite_max(ex[both]),
-        "max_err_obj": _finite_max(eo[both]),
-        "max_err_grad": _finite_max(eg[both]),
-        "conv_mismatch": int((np.asarray(gpu_conv) != ref["conv"]).sum()),
-        "iters_mismatch": int((np.asarray(gpu_iters) != ref["iters"]).sum()),
-        "reference_not_converged": int((ref["conv"] != 1).sum()),
-    }
-    return fig, ref
+    return _figures(B, gpu_conv, gpu_iters, ex, eo, eg, ref, g_bar), ref
 
 
-def elastic(data, penalty, tol, kappa, dl, gpu_out, gpu_grads, ref=None):
+def elastic(data, penalty, tol, kappa, dl, gpu_out, gpu_grads, ref=None, perturb=0, g_bar=1e-5):
     """Parity of solve_qp_elastic_primal forward + backward: x and the slacks
     (t, s1, s2) as the elastic configuration compares them, the objective
     (with the penalty term) and the four gradients, for incoming gradient dl."""
     Q, q, G, h = data
     B = np.asarray(q).shape[0]
+
+    def run(d):
+        out = oracle.solve_qp_elastic(*d, penalty, solver_tol=tol)
+        _, grads = oracle.solve_qp_elastic_primal_vjp(*d, penalty, dl, solver_tol=tol, target_kappa=kappa)
+        return dict(out=out, grads=grads, conv=np.asarray(out[6]), iters=np.asarray(out[7]))
+
     if ref is None:
-        out = oracle.solve_qp_elastic(Q, q, G, h, penalty, solver_tol=tol)
-        _, grads_o = oracle.solve_qp_elastic_primal_vjp(Q, q, G, h, penalty, dl, solver_tol=tol, target_kappa=kappa)
-        ref = dict(out=out, grads=grads_o, conv=np.asarray(out[6]), iters=np.asarray(out[7]))
-    gconv = np.asarray(gpu_out[6])
-    both = (gconv == 1) & (ref["conv"] == 1)
+        ref = run(data)
+    if perturb and "stable" not in ref:
+        runs = [run(perturb_inputs(data, 1e-15, 2000 + k)) for k in range(perturb)]
+        ref["stable"] = np.all([(r["conv"] == ref["conv"]) & (r["iters"] == ref["iters"]) for r in runs], axis=0)
+        ref["grad_stable"] = ref["stable"] & (_spread(ref, runs, B, "grads") <= 0.1 * g_bar)
+        ref["perturbed_runs"] = perturb
     ex = np.zeros(B)
     for k in range(4):  # x, t, s1, s2
         ex = np.maximum(ex, rel_errors(gpu_out[k], ref["out"][k], B))
@@ -100,14 +175,4 @@ def elastic(data, penalty, tol, kappa, dl, gpu_out, gpu_grads, ref=None):
     eg = np.zeros(B)
     for g, go in zip(gpu_grads, ref["grads"]):
         eg = np.maximum(eg, rel_errors(g, go, B))
-    fig = {
-        "instances": int(B),
-        "compared": int(both.sum()),
-        "max_err_x": _finite_max(ex[both]),
-        "max_err_obj": _finite_max(eo[both]),
-        "max_err_grad": _finite_max(eg[both]),
-        "conv_mismatch": int((gconv != ref["conv"]).sum()),
-        "iters_mismatch": int((np.asarray(gpu_out[7]) != ref["iters"]).sum()),
-        "reference_not_converged": int((ref["conv"] != 1).sum()),
-    }
-    return fig, ref
+    return _figures(B, gpu_out[6], gpu_out[7], ex, eo, eg, ref, g_bar), ref

