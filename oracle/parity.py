@@ -116,6 +116,28 @@ def _figures(B, gpu_conv, gpu_iters, ex, eo, eg, ref, g_bar):
     return fig
 
 
+def forward(data, tol, gpu_x, gpu_conv, gpu_iters, perturb=2):
+    """Parity of a solve_qp forward alone (figures as standard(), without
+    gradients): x and the objective where both converged, converged flags and
+    iteration counts where the reference outcome is reproducible."""
+    Q, q, A, b, G, h = data
+    B = len(q) if isinstance(q, (list, tuple)) else np.asarray(q).shape[0]
+
+    def run(d):
+        out = oracle.solve_qp(*d, solver_tol=tol)
+        return dict(x=out[0], conv=np.asarray(out[4]), iters=np.asarray(out[5]))
+
+    ref = run(data)
+    runs = [run(perturb_inputs(data, 1e-15, 3000 + k)) for k in range(perturb)]
+    ref["stable"] = np.all([(r["conv"] == ref["conv"]) & (r["iters"] == ref["iters"]) for r in runs], axis=0)
+    ref["grad_stable"] = ref["stable"]
+    ref["perturbed_runs"] = perturb
+    ex = rel_errors(gpu_x, ref["x"], B)
+    fo, fg = objective(Q, q, ref["x"], B), objective(Q, q, gpu_x, B)
+    eo = np.abs(fg - fo) / np.maximum(1.0, np.abs(fo))
+    return _figures(B, gpu_conv, gpu_iters, ex, eo, np.zeros(B), ref, 1e-5)
+
+
 def standard(data, tol, kappa, dl, gpu_x, gpu_conv, gpu_iters, gpu_grads, ref=None, perturb=0, g_bar=1e-5):
     """Parity of a solve_qp_primal forward + backward against the oracle.
 

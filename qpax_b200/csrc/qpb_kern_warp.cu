@@ -8,14 +8,14 @@ namespace qpb {
 
 // kWarps instances per CTA; kMinBlocks bounds registers so that the register
 // file does not cap residency below what shared memory allows.
-template <int NP, int MP, int kMinBlocks, unsigned kOpt = 0>
+template <int NP, int MP, int kMinBlocks>
 __global__ void __launch_bounds__(kWarpKernelThreads, kMinBlocks) warp_kernel(const __grid_constant__ Params P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int team = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   unsigned char* arena = P.arena_in_smem ? smem + (size_t)team * P.arena_bytes
                                          : P.arena + ((size_t)blockIdx.x * (blockDim.x >> 5) + team) * P.arena_bytes;
-  WarpQP<NP, MP, kOpt> S;
+  WarpQP<NP, MP> S;
   S.setup(P, arena, lane);
   for (;;) {
     int v = 0;

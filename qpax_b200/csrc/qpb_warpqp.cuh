@@ -10,9 +10,9 @@
 //     (scaled by d_j) below the diagonal and row j of L (scaled by d_i) above
 //     it, which is exactly what column-oriented forward and backward
 //     substitution need from that lane;
-//   * Y = L^-1 A' is formed in registers (lane j holds Y[:, j]) and kept in
-//     shared memory with the m x m Schur complement F = Y' D^-1 Y and its
-//     factor;
+//   * Y = L^-1 A' is formed inside the same elimination loop (lane j holds
+//     row j of Y) and kept in shared memory with the m x m Schur complement
+//     F = Y' D^-1 Y (one FP64 tensor-core tile) and its register-factored LDL^T;
 //   * n- and m-vectors are lane-distributed registers; p-vectors and the G,
 //     A operands live in shared memory; Q is read through L1/L2.
 // Every solve of the instance -- initial point, predictor, corrector, Newton
@@ -82,19 +82,7 @@ struct WarpAddr {
   QPB_DEV double* F() const { return Y() + (MP > 8 ? MP : 8) * (NP + 1); }
 };
 
-// Code-shape options of the warp kernel (bit set).
-enum WarpOpt : unsigned {
-  kWoFReg = 1,    // factor the m x m Schur complement F in registers
-  kWoFuseY = 2,   // form Y = L^-1 A' inside the LDL^T loop
-  kWoOneFma = 4,  // LDL^T update as one FMA per element (l = S[k][j] / d_k)
-  kWoXsm = 8,     // residuals: x broadcast through shared memory for Q x
-  kWoHpre = 16,   // H formation k-loop unrolled by two
-  kWoVecLds = 32, // LDL^T: pivot row read as 16-byte pairs
-  kWoH1 = 64,     // H formation: all lower tiles in one pass over G
-  kWoFdmma = 128  // F = Y' D^-1 Y on the FP64 tensor cores
-};
-
-template <int NP, int MP, unsigned kOpt = 0>
+template <int NP, int MP>
 struct WarpQP {
   static_assert(NP == 8 || NP == 16 || NP == 32, "NP");
   static constexpr int kYld = NP + 1;  // row stride of Y
@@ -293,37 +281,11 @@ struct WarpQP {
     __syncwarp();
   }
 
-  // hc[i] += (G' diag(w) G)[i][lane].  The lower-triangle 8x8 tiles are
-  // accumulated one tile row at a time on the FP64 tensor cores
-  // (H_tile(ti, tj) = sum_k (w_k G[k][8ti..]) (x) G[k][8tj..]).
-  template <int TI>
-  QPB_DEV void h_tile_row() {
-    const int g = lane >> 2, t = lane & 3;
-    const double* Gs = a.G();
-    const double* wv = a.w();
-    const int kblocks = (p + 3) >> 2;
-    double acc[TI + 1][2];
-#pragma unroll
-    for (int tj = 0; tj <= TI; ++tj) acc[tj][0] = acc[tj][1] = 0.0;
-    const int sw = gswz(t);  // = gswz(4 kb + t)
-#pragma unroll((kOpt & kWoHpre) ? 2 : 1)
-    for (int kb = 0; kb < kblocks; ++kb) {
-      const int k = 4 * kb + t;
-      const bool in = k < p;
-      const double* row = Gs + (in ? k : 0) * NP;
-      const double a0 = in ? wv[k] * row[(8 * TI + g) ^ sw] : 0.0;  // (diag(w) G)'[8TI+g][k]
-#pragma unroll
-      for (int tj = 0; tj <= TI; ++tj) {
-        const double b0 = in ? row[(8 * tj + g) ^ sw] : 0.0;  // G[k][8tj+g]
-        dmma884(acc[tj][0], acc[tj][1], a0, b0);
-      }
-    }
-    scatter_tile_row<TI>(acc);
-  }
-
-  // All lower tiles in one pass over G: each k-step loads the NP/8 fragments
-  // once and feeds every tile (the same operands and accumulation order per
-  // tile as h_tile_row, so the same H bit for bit).
+  // hc[i] += (G' diag(w) G)[i][lane]: the lower-triangle 8x8 tiles
+  // H_tile(ti, tj) = sum_k (w_k G[k][8ti..]) (x) G[k][8tj..] on the FP64
+  // tensor cores, all in one pass over G (each k-step loads the NP/8
+  // fragments once and feeds every tile), then scattered one tile row at a
+  // time.
   QPB_DEV void form_h_onepass() {
     constexpr int T = NP / 8;
     const int g = lane >> 2, t = lane & 3;
@@ -367,18 +329,8 @@ struct WarpQP {
   }
 
   // Adds G' diag(w) G to hc (each element of the column exactly once).
-  QPB_DEV void form_h_tensor() {
-    if constexpr ((kOpt & kWoH1) != 0) {
-      form_h_onepass();
-    } else {
-      h_tile_row<0>();
-      if constexpr (NP > 8) h_tile_row<1>();
-      if constexpr (NP > 16) {
-        h_tile_row<2>();
-        h_tile_row<3>();
-      }
-    }
-  }
+  QPB_DEV void form_h_tensor() { form_h_onepass(); }
+
 
   // ---------------------------------------------------------------- factor
   // H = sym(Q) + G' diag(w) G (w in shared memory), LDL^T in registers,
@@ -397,23 +349,21 @@ struct WarpQP {
 #pragma unroll
       for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qv[i] + hc[i];
     }
-    // LDL^T: step k broadcasts row k of the Schur complement (= column k)
+    // LDL^T: step k broadcasts row k of the Schur complement (= column k);
+    // Y = L^-1 A' is formed in the same loop: lane j holds Y[j][0..MP), and
+    // step k broadcasts lane k's (final) row of Y beside the pivot row.
     int bad = 0;
-    double* cb = a.cb();
+    double* cb = a.cb();  // 16-byte aligned (WarpArena pads it)
+    double* yb = a.Y();   // free until Y is stored below
     double yc[MP];
-    double* yb = a.Y();  // fused Y: lane k's column of Y (free until Y is stored)
-    if constexpr ((kOpt & kWoFuseY) != 0) {
 #pragma unroll
-      for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
-    }
+    for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       if (lane < NP) cb[lane] = hc[k];
-      if constexpr ((kOpt & kWoFuseY) != 0) {
-        if (lane == k) {
+      if (lane == k) {
 #pragma unroll
-          for (int i = 0; i < MP; ++i) yb[i] = yc[i];
-        }
+        for (int i = 0; i < MP; ++i) yb[i] = yc[i];
       }
       __syncwarp();
       const double dk = cb[k];
@@ -422,67 +372,35 @@ struct WarpQP {
       if (lane == k) dinv = rk;
       // S[i][j] -= (S[k][i] * S[k][j]) / d_k: the product is formed the same
       // way for (i, j) and (j, i), so both triangles stay bit-identical and the
-      // row-held and column-held copies of L agree exactly.
+      // row-held and column-held copies of L agree exactly.  The pivot row is
+      // read in 16-byte pairs.
       const double hk = hc[k];
       if (lane > k) {
-        if constexpr ((kOpt & kWoOneFma) != 0) {
-          const double l = hk * rk;
-          if constexpr ((kOpt & kWoVecLds) != 0) {
-            if ((k + 1) & 1) hc[k + 1] = fma(-cb[k + 1], l, hc[k + 1]);
+        if ((k + 1) & 1) hc[k + 1] = fma(-(cb[k + 1] * hk), rk, hc[k + 1]);
 #pragma unroll
-            for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
-              const double2 c2 = *reinterpret_cast<const double2*>(cb + i2);
-              hc[i2] = fma(-c2.x, l, hc[i2]);
-              hc[i2 + 1] = fma(-c2.y, l, hc[i2 + 1]);
-            }
-          } else {
-#pragma unroll
-            for (int i = k + 1; i < NP; ++i) hc[i] = fma(-cb[i], l, hc[i]);
-          }
-        } else if constexpr ((kOpt & kWoVecLds) != 0) {
-          if ((k + 1) & 1) hc[k + 1] = fma(-(cb[k + 1] * hk), rk, hc[k + 1]);
-#pragma unroll
-          for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
-            const double2 c2 = *reinterpret_cast<const double2*>(cb + i2);
-            hc[i2] = fma(-(c2.x * hk), rk, hc[i2]);
-            hc[i2 + 1] = fma(-(c2.y * hk), rk, hc[i2 + 1]);
-          }
-        } else {
-#pragma unroll
-          for (int i = k + 1; i < NP; ++i) hc[i] = fma(-(cb[i] * hk), rk, hc[i]);
+        for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
+          const double2 c2 = *reinterpret_cast<const double2*>(cb + i2);
+          hc[i2] = fma(-(c2.x * hk), rk, hc[i2]);
+          hc[i2 + 1] = fma(-(c2.y * hk), rk, hc[i2 + 1]);
         }
-        if constexpr ((kOpt & kWoFuseY) != 0) {
-          const double l = hk * rk;  // = L[lane][k], as the separate Y loop forms it
+        const double l = hk * rk;  // L[lane][k]
 #pragma unroll
-          for (int i = 0; i < MP; ++i) yc[i] = fma(-l, yb[i], yc[i]);
-        }
+        for (int i = 0; i < MP; ++i) yc[i] = fma(-l, yb[i], yc[i]);
       }
       __syncwarp();
     }
     if (lane < NP) a.dvi()[lane] = dinv;
-    __syncwarp();
-    if constexpr ((kOpt & kWoFuseY) == 0) {
-      // Y = L^-1 A'   (unit L; L[j][k] = hc[k] * dinv_k for lane j > k)
-#pragma unroll
-      for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? a.A()[i * NP + lane] : 0.0;
-#pragma unroll
-      for (int k = 0; k < NP - 1; ++k) {
-        const double l = (lane > k && lane < NP) ? hc[k] * a.dvi()[k] : 0.0;
-#pragma unroll
-        for (int i = 0; i < MP; ++i) yc[i] = fma(-l, __shfl_sync(kFull, yc[i], k), yc[i]);
-      }
-    }
     if (lane < NP) {
 #pragma unroll
       for (int i = 0; i < MP; ++i) a.Y()[i * kYld + lane] = yc[i];
     }
     __syncwarp();
-    // F = Y D^-1 Y' (MP x MP, full storage, identity beyond m), one entry per lane
+    // F = Y' D^-1 Y (MP x MP, identity beyond m) on the FP64 tensor cores: one
+    // 8 x 8 tile, F[g][c] = sum_j (Y[j][g] dinv_j) Y[j][c], four j per step
     double* Fm = a.F();
-    const double* Ys = a.Y();
-    const double* dv = a.dvi();
-    if constexpr ((kOpt & kWoFdmma) != 0) {
-      // one 8 x 8 tile: F[g][c] = sum_j (Y[j][g] dinv_j) Y[j][c], four j per step
+    {
+      const double* Ys = a.Y();
+      const double* dv = a.dvi();
       const int g = lane >> 2, t = lane & 3;
       double f0 = 0.0, f1 = 0.0;
 #pragma unroll
@@ -498,22 +416,11 @@ struct WarpQP {
           if (c < MP) Fm[g * MP + c] = (g < m && c < m) ? (u ? f1 : f0) : (g == c ? 1.0 : 0.0);
         }
       }
-    } else
-    for (int e = lane; e < MP * MP; e += 32) {
-      const int r = e / MP, c = e - r * MP;
-      double v = (r == c) ? 1.0 : 0.0;
-      if (r < m && c < m) {
-        double acc = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < NP; ++j) acc = fma(Ys[r * kYld + j] * dv[j], Ys[c * kYld + j], acc);
-        v = acc;
-      }
-      Fm[e] = v;
     }
     __syncwarp();
-    if constexpr ((kOpt & kWoFReg) != 0) {
-      // LDL^T of F in registers, lane c owning column c; step k broadcasts
-      // column k (the operands and order of the shared-memory form below)
+    // LDL^T of F in registers, lane c owning column c; step k broadcasts
+    // column k; the factor goes back to shared memory (the solves read it)
+    {
       double fc[MP];
 #pragma unroll
       for (int i = 0; i < MP; ++i) fc[i] = (lane < MP) ? Fm[i * MP + lane] : 0.0;
@@ -541,19 +448,6 @@ struct WarpQP {
         for (int i = 0; i < MP; ++i) Fm[i * MP + lane] = fc[i];
       }
       __syncwarp();
-    } else {
-      // LDL^T of F in the same in-place layout as H: lane c owns column c
-      for (int k = 0; k < MP; ++k) {
-        const double dk = Fm[k * MP + k];
-        const double rk = 1.0 / dk;
-        if (k < m) bad |= !(dk > 0.0) || !isfinite(dk);
-        if (lane == k) fdinv = rk;
-        if (lane > k && lane < MP) {
-          const double f = Fm[k * MP + lane] * rk;
-          for (int i = k + 1; i < MP; ++i) Fm[i * MP + lane] = fma(-Fm[i * MP + k], f, Fm[i * MP + lane]);
-        }
-        __syncwarp();
-      }
     }
     if (bad) st_flags |= kFlagBreakdown64;
   }
@@ -675,19 +569,14 @@ struct WarpQP {
   // qpax/pdip.py:93-100, pdip_relaxed.py:16-23.
   QPB_DEV double residuals(double kappa, double& v1, double& v4) {
     double qx = 0.0;
-    if constexpr ((kOpt & kWoXsm) != 0) {
-      if (lane < NP) a.xs()[lane] = x;
-      __syncwarp();
+    if (lane < NP) a.xs()[lane] = x;  // x broadcast for Q x (and G x below)
+    __syncwarp();
+    {
       double qv[NP];
       load_q(qv);
       const double* xsv = a.xs();
 #pragma unroll
       for (int i = 0; i < NP; ++i) qx = fma(qv[i], xsv[i], qx);
-    } else {
-      double qv[NP];
-      load_q(qv);
-#pragma unroll
-      for (int i = 0; i < NP; ++i) qx = fma(qv[i], __shfl_sync(kFull, x, i), qx);
     }
     double ay = 0.0;
 #pragma unroll
@@ -695,8 +584,6 @@ struct WarpQP {
     const double r1 = ((qx + q) + ay) + gcol_dot(a.z());
     double loc = (lane < n) ? fabs(r1) : 0.0;
     v1 = (lane < n) ? -r1 : 0.0;
-    if (lane < NP) a.xs()[lane] = x;
-    __syncwarp();
     double r4 = 0.0;
 #pragma unroll
     for (int i = 0; i < MP; ++i) {
