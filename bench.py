@@ -379,8 +379,11 @@ class UniformArm:
         from oracle import parity
 
         dl = self.gx.cpu().numpy()
-        return parity.standard(data, self.spec.tol, KAPPA, dl, self.x.cpu().numpy(), self.conv.cpu().numpy(),
-                               self.iters.cpu().numpy(), [g.cpu().numpy() for g in self.grads], perturb=2)[0]
+        gpu = dict(x=self.x.cpu().numpy(), s=self.s.cpu().numpy(), z=self.z.cpu().numpy(), y=self.y.cpu().numpy(),
+                   conv=self.conv.cpu().numpy(), iters=self.iters.cpu().numpy(), riters=self.riters.cpu().numpy(),
+                   grads=[g.cpu().numpy() for g in self.grads])
+        eps = 1e-12 if self.opts.get("precision") == "mixed" else 1e-15
+        return parity.standard(data, self.spec.tol, KAPPA, dl, gpu, perturb=2, eps=eps)[0]
 
     def kernel_name(self, which):
         return "qpb_solve_qp (forward)" if which == "forward" else "qpb_solve_qp_primal_bwd (backward)"
@@ -455,9 +458,10 @@ class ElasticArm:
     def parity(self, data, limit=None):
         from oracle import parity
 
+        eps = 1e-12 if self.opts.get("precision") == "mixed" else 1e-15
         return parity.elastic(tuple(data), 1e3, self.spec.tol, KAPPA, self.gx.cpu().numpy(),
                               [t.cpu().numpy() for t in self.out], [g.cpu().numpy() for g in self.grads], perturb=2,
-                              g_bar=1e-4)[0]
+                              eps=eps, g_bar=1e-4)[0]
 
     def kernel_name(self, which):
         return ("qpb_solve_qp_elastic (forward)" if which == "forward"
@@ -476,7 +480,8 @@ class UnevenArm:
 
         self.spec = spec
         n, m, p = shapes_of(spec, data)
-        self.plan = PackedPlan(list(zip(n, m, p)), precision=opts.get("precision") or "auto",
+        self.precision = opts.get("precision") or "auto"
+        self.plan = PackedPlan(list(zip(n, m, p)), precision=self.precision,
                                team_threads=opts.get("team_threads") or 0)
         self.ins = [pack(v, dev) for v in data]
         if opts.get("tune"):
@@ -533,9 +538,11 @@ class UnevenArm:
         L = self.plan.lengths
         cut = lambda t, f: [v.cpu().numpy() for v in unpack(t, L[f])[:k]]
         sub = [v[:k] for v in data]
-        fig = parity.standard(sub, self.spec.tol, KAPPA, cut(self.gx, 1), cut(self.out[0], 1),
-                              self.out[4][:k].cpu().numpy(), self.out[5][:k].cpu().numpy(),
-                              [cut(self.grads[f], f) for f in range(6)], perturb=2)[0]
+        gpu = dict(x=cut(self.out[0], 1), s=cut(self.out[1], 5), z=cut(self.out[2], 5), y=cut(self.out[3], 3),
+                   conv=self.out[4][:k].cpu().numpy(), iters=self.out[5][:k].cpu().numpy(),
+                   riters=self.riters[:k].cpu().numpy(), grads=[cut(self.grads[f], f) for f in range(6)])
+        fig = parity.standard(sub, self.spec.tol, KAPPA, cut(self.gx, 1), gpu, perturb=2,
+                              eps=1e-12 if self.precision == "mixed" else 1e-15)[0]
         fig["sample"] = f"the first {k} instances of the batch"
         return fig
 
@@ -680,9 +687,11 @@ def run_ours(args, spec: Spec, world, rank, local):
         line["parity"]["against"] = ("the FP64 oracle (C restatement of qpax) on the same inputs and the same dl/dx, "
                                      "computed after the timed steps; errors relative per instance, "
                                      "||gpu - ref||_inf / max(1, ||ref||_inf); objective 1/2 x'Qx + q'x; "
+                                     "gpu_only_converged: instances where qpax's QR-based solve breaks down and the "
+                                     "GPU converges (gpu_only_max_kkt: KKT residual of the GPU's returned iterate); "
                                      "'reproducible' = the oracle gives the same flag and iteration count (and a "
                                      "gradient within a tenth of the 1e-5 bar) on two runs with inputs perturbed by "
-                                     "1e-15 relative")
+                                     "1e-15 relative (1e-12 for the mixed variant, whose solves are refined to 1e-12)")
     if not args.no_e2e:  # every rank takes part (barriers, max over ranks)
         e2e = run_e2e(args, spec, data, dev, arm_main, world)
         if rank == 0:
@@ -713,6 +722,7 @@ def run_configs(args, world, rank, dev, stream, flush):
         tot, fwd_ms, bwd_ms = time_arm(args, arm, stream, flush, world, steps)
         conv, iters, riters = arm.counts()
         entry = {"workload": spec.workload, "metric": metric_for(spec),
+                 "launch_shapes": arm.plan.bin_info() if hasattr(arm, "plan") else None,
                  "value": world * spec.batch * steps / (tot * 1e-3), "unit": "QPs/s", "steps": steps,
                  "ms_per_step": tot / steps, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                  "iterations": {"forward_mean": float(iters.mean()), "relax_mean": float(riters.mean()),

@@ -288,6 +288,11 @@ int qpb_solve_qp_noalloc(const qpb_dims* dims, const double* Q, const double* q,
  * qpb_solve_qp_primal_vjp_host_workspace_size bytes (256-byte aligned).
  * Everything is enqueued after the work already on `stream`, and `stream`
  * waits for all of it: synchronize `stream` before reading the outputs.
+ * The internal streams are created once per device and shared by every call
+ * on that device: calls from several host threads are safe when each has
+ * its own workspace, but their chunks are queued on the same streams and
+ * interleave in enqueue order -- concurrent calls share the streams rather
+ * than running side by side.
  * Requires p >= 1. */
 size_t qpb_solve_qp_primal_vjp_host_workspace_size(const qpb_dims* dims, int32_t chunks, const qpb_config* cfg);
 int qpb_solve_qp_primal_vjp_host(const qpb_dims* dims, const double* Q, const double* q, const double* A,
