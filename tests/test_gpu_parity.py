@@ -286,6 +286,29 @@ def test_autograd_matches_vjp():
         np.testing.assert_allclose(np_(t.grad), np_(g), rtol=0, atol=1e-12)
 
 
+def test_autograd_with_host_inputs():
+    """Inputs on the host (CPU float64, requires_grad) go through the GPU and
+    come back with their gradients on the host, equal to the CUDA-input case
+    (solve_qp_primal and solve_qp_elastic_primal)."""
+    import qpax_b200 as qb
+
+    Q, q, A, b, G, h = wl.dense(8, 12, 3, 24, 23)
+    cpu = [torch.tensor(a, requires_grad=True) for a in (Q, q, A, b, G, h)]
+    dev = [torch.tensor(a, device="cuda", requires_grad=True) for a in (Q, q, A, b, G, h)]
+    for ts in (cpu, dev):
+        x = qb.solve_qp_primal(*ts, solver_tol=1e-6, target_kappa=1e-3)
+        ((x - 1.0) ** 2).sum().backward()
+    for c, d in zip(cpu, dev):
+        assert c.grad is not None and c.grad.device.type == "cpu" and c.grad.dtype == torch.float64
+        np.testing.assert_array_equal(c.grad.numpy(), np_(d.grad))
+    Qe, qe, Ge, he, _ = wl.elastic(4, seed=3, n=10, p=20, pairs=2)
+    cpu = [torch.tensor(a, requires_grad=True) for a in (Qe, qe, Ge, he)]
+    x = qb.solve_qp_elastic_primal(*cpu, 50.0, solver_tol=1e-6, target_kappa=1e-3)
+    x.sum().backward()
+    for c in cpu:
+        assert c.grad is not None and c.grad.device.type == "cpu" and c.grad.shape == c.shape
+
+
 @pytest.mark.parametrize("team", [32, 128])
 def test_team_sizes_agree(team):
     """Warp-per-instance and CTA-per-instance teams give the oracle's answer."""
