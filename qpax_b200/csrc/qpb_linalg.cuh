@@ -157,6 +157,78 @@ QPB_NOINLINE void form_H_dmma(const Team<NT>& t, int n, int p, const double* Q, 
   }
 }
 
+// FP32 H = sym(Q) + GS' GS on the tensor cores for the mixed path (n >= 64),
+// GS = float(sqrt(w) G): 16 x 8 tiles of the lower triangle, one warp per
+// tile, mma.m16n8k8 over TF32 operands in the 3xTF32 split (x = big + small,
+// both TF32; big*big + big*small + small*big accumulated in FP32, small
+// products first), which keeps about FP32 accuracy.  Fragments (PTX
+// m16n8k8 .tf32): a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4];
+// b = B[t][g], B[t+4][g]; d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]
+// with g = lane / 4, t = lane % 4.  A = GS' (row r, column k = GS[k][r]).
+QPB_DEV unsigned tf32_big(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+QPB_DEV void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <int NT>
+QPB_NOINLINE void form_H_tf32(const Team<NT>& t, int n, int p, const double* Q, int ldq, const float* GS, int ldg,
+                              float* H, int ldh) {
+  const int rb = (n + 15) >> 4, cb = (n + 7) >> 3;
+  // tiles (bi, bj) with 8 bj < 16 (bi + 1): the 16-row blocks of the lower triangle
+  int ntiles = 0;
+  for (int bi = 0; bi < rb; ++bi) ntiles += min(2 * bi + 2, cb);
+  const int lane = t.lane(), g = lane >> 2, tg = lane & 3;
+  for (int tau = t.warp(); tau < ntiles; tau += NT / 32) {
+    int bi = 0, rem = tau;
+    while (rem >= min(2 * bi + 2, cb)) {
+      rem -= min(2 * bi + 2, cb);
+      ++bi;
+    }
+    const int bj = rem;
+    const int r0 = 16 * bi + g, r1 = r0 + 8, cj = 8 * bj + g;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k0 = 0; k0 < p; k0 += 8) {
+      const int ka = k0 + tg, kb = ka + 4;
+      const float* ra = GS + (size_t)(ka < p ? ka : 0) * ldg;
+      const float* rbp = GS + (size_t)(kb < p ? kb : 0) * ldg;
+      const float av[4] = {(ka < p && r0 < n) ? ra[r0] : 0.f, (ka < p && r1 < n) ? ra[r1] : 0.f,
+                           (kb < p && r0 < n) ? rbp[r0] : 0.f, (kb < p && r1 < n) ? rbp[r1] : 0.f};
+      const float bv[2] = {(ka < p && cj < n) ? ra[cj] : 0.f, (kb < p && cj < n) ? rbp[cj] : 0.f};
+      unsigned abig[4], asml[4], bbig[2], bsml[2];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        abig[e] = tf32_big(av[e]);
+        asml[e] = tf32_big(av[e] - __uint_as_float(abig[e]));
+      }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        bbig[e] = tf32_big(bv[e]);
+        bsml[e] = tf32_big(bv[e] - __uint_as_float(bbig[e]));
+      }
+      mma_tf32(d, abig, bsml);
+      mma_tf32(d, asml, bbig);
+      mma_tf32(d, abig, bbig);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = (e < 2) ? r0 : r1;
+      const int j = 8 * bj + 2 * tg + (e & 1);
+      if (i < n && j <= i) {
+        const double qs = 0.5 * (Q[(size_t)i * ldq + j] + Q[(size_t)j * ldq + i]);
+        H[(size_t)i * ldh + j] = (float)qs + d[e];
+      }
+    }
+  }
+}
+
 // Factor the reduced KKT matrix for weights wv.  G, A are n4-padded FP64.
 // For R == float, GS (p x ldg floats) is scratch for sqrt(w)-scaled G.
 // Returns the H pivot ratio (+inf when the factor is unusable) to all threads.
@@ -169,7 +241,10 @@ QPB_NOINLINE double factor_kkt(const Team<NT>& t, int n, int m, int p, const dou
       GS[e] = (float)(sqrt(wv[k]) * G[e]);
     }
     t.sync();
-    form_H<NT, float, float, false>(t, n, p, Q, ld, GS, ld, wv, f.L, f.ldl);
+    if (n >= 64)  // GS' GS on the tensor cores (3xTF32) for the larger size bins
+      form_H_tf32<NT>(t, n, p, Q, ld, GS, ld, f.L, f.ldl);
+    else
+      form_H<NT, float, float, false>(t, n, p, Q, ld, GS, ld, wv, f.L, f.ldl);
   } else {
     form_H_dmma<NT>(t, n, p, Q, ld, G, ld, wv, f.L, f.ldl);
   }
