@@ -71,7 +71,7 @@ typedef struct {
   int32_t precision;    /* qpb_precision; default QPB_PRECISION_AUTO */
   int32_t team_threads; /* threads per instance: 0 = automatic, 32, 128 or 256
                            (128/256 force the one-CTA-per-instance kernel) */
-  double pivot_max;     /* mixed: FP32 factor used while max(d)/min(d) <= pivot_max (0 = 1e5) */
+  double pivot_max;     /* mixed: FP32 factor used while max(d)/min(d) <= pivot_max (0 = 1e7) */
   int32_t max_sweeps;   /* mixed: FP64 refinement sweeps per solve before FP64 refactor (0 = 8) */
   int32_t* stats;       /* optional device int32[batch][4]: FP32 factorisations, FP64
                            factorisations, refinement sweeps, flag bits (1 FP32 factor

@@ -399,7 +399,7 @@ int tune_pick(Params P, int op, const qpb_dims& d, const qpb_config& cfg, void* 
 qpb_config resolve_config(const qpb_config* c) {
   qpb_config r{};
   if (c) r = *c;
-  if (r.pivot_max <= 0) r.pivot_max = 1e5;
+  if (r.pivot_max <= 0) r.pivot_max = 1e7;  // FP64 refactor above a pivot ratio of 1e7
   if (r.max_sweeps <= 0) r.max_sweeps = 8;
   return r;
 }
