@@ -3,7 +3,9 @@
 Bars (written per assertion):
   x, s, z, y, t, s1, s2, z1, z2: ||gpu - oracle||_inf <= 1e-6 * max(1, ||oracle||_inf) per instance
   gradients:                     ||gpu - oracle||_inf <= 1e-5 * max(1, ||oracle||_inf) per instance and array
-  converged flags:               identical; iteration counts: identical
+  converged flags, iteration counts: identical wherever the reference converges
+                                 (where qpax's own method breaks down, the GPU may
+                                 converge: checked by its KKT residual)
 for each kernel family:
   "auto":     the default dispatch (one warp per instance in FP64 for n <= 32, m <= n_pad/4,
               one CTA per instance in FP64 above)
@@ -61,20 +63,27 @@ def assert_close(gpu, ref, tol, what):
 
 
 def check_solve(Q, q, A, b, G, h, tol, prec, max_breakdown=0.0, **kw):
-    """Converged flags identical on every instance; outputs and iteration
-    counts compared on every instance qpax's method converges on.  Where the
-    FP64 reference itself breaks down (its residual reaches ~tol, then grows
-    until the 30-iteration cap: ill-conditioned H late in the loop), the GPU
-    must not converge either; the trajectory after the breakdown is set by
-    rounding and is not compared.  The share of such instances is bounded by
-    max_breakdown."""
+    """Every instance qpax's method solves is solved, in the same number of
+    iterations, with x, s, z, y within X_TOL.  Where the FP64 reference
+    itself breaks down (its QR-based solve loses accuracy at cond ~1e14+ late
+    in the loop: the residual grows until the 30-iteration cap), the GPU may
+    converge too -- its returned iterate must then satisfy the KKT conditions
+    to 100 x tol (the flag refers to the iterate before qpax's final step);
+    those trajectories are set by rounding and are not compared.  The share
+    of reference breakdowns is bounded by max_breakdown."""
     import qpax_b200 as qb
 
     out = qb.solve_qp(Q, q, A, b, G, h, tol, **VARIANTS[prec], **kw)
     ref = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=tol)
     ok = np.atleast_1d(ref[4]) == 1
     assert (~ok).mean() <= max_breakdown, f"reference breakdowns {(~ok).sum()} of {ok.size}"
-    np.testing.assert_array_equal(np.atleast_1d(np_(out[4])), np.atleast_1d(ref[4]), err_msg="converged flags")
+    conv = np.atleast_1d(np_(out[4]))
+    np.testing.assert_array_equal(conv[ok], 1, err_msg="converged flags")
+    gpu_only = (conv == 1) & ~ok
+    if gpu_only.any():
+        outs = [np.asarray(np_(t)).reshape(conv.size, -1) for t in out[:4]]
+        kkt = kkt_inf_norms(Q, q, A, b, G, h, *outs).max(axis=1)  # batched inputs
+        assert kkt[gpu_only].max() <= 100 * tol, kkt[gpu_only]
     np.testing.assert_array_equal(np.atleast_1d(np_(out[5]))[ok], np.atleast_1d(ref[5])[ok],
                                   err_msg="iteration counts")
     for k, name in enumerate("xszy"):
@@ -441,7 +450,12 @@ def test_stats_count_factorisations():
     _, _, _, _, conv, iters = qb.solve_qp(Q, q, A, b, G, h, 1e-6, precision="mixed", stats=stats)
     st = np_(stats)
     total = st[:, 0] + st[:, 1]
-    np.testing.assert_array_equal(total, np_(iters) + 1)  # one per iteration + the initial point
+    # one per iteration + the initial point, plus one FP64 refactor where
+    # refinement against an accepted FP32 factor stalled (flag 2; the
+    # instance stays on FP64 factors afterwards)
+    stalled = (st[:, 3] & 2) != 0
+    np.testing.assert_array_equal(total, np_(iters) + 1 + stalled)
+    assert (st[:, 0] > 0).all() and (st[:, 2] > 0).all()  # FP32 factors served solves, with refinement
     stats.zero_()
     qb.solve_qp(Q, q, A, b, G, h, 1e-6, precision="fp64", stats=stats)
     assert (np_(stats)[:, 0] == 0).all()
