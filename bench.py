@@ -8,18 +8,27 @@ solver_tol 1e-6, target_kappa 1e-3, loss ||x - 1||^2:
   backward = qpb_solve_qp_primal_bwd (relaxation to kappa + adjoint KKT solve
              + the six gradient outer products)
 Inputs are resident in HBM; L2 is flushed (256 MB write) between steps,
-outside the per-step CUDA events.  Synthetic seeded data (no dataset).
+outside the per-step CUDA events.  Launch shapes are autotuned at setup
+(untimed).  Synthetic seeded data (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload dense|nnls|small|uneven|elastic] [--batch B]
+                    [--no-e2e] [--no-cpu] [--no-parity] [--no-tune] [--no-configs]
+                    [--only-default] [--e2e-chunks C] [--config-steps K]
 
-Other workloads (same JSON line, `config.workload` names them):
+The JSON line carries the default path's `value`, the plain FP64
+one-CTA-per-QP and mixed variants (`variants`, `mixed_over_plain_fp64`),
+`parity` against the FP64 oracle per variant (computed after the timed
+steps), `e2e` from pinned host buffers, `roofline`, `cpu_baseline`, and for
+the dense workload a `configs` block with the other four configurations
+(value, e2e, parity each):
   nnls     10000 non-negative least squares QPs, n = 5, G = -I, no equalities
   small    2048 dense QPs n = 16, m = 4, p = 32, solver_tol 1e-5
   uneven   16384 QPs of different sizes: n ~ U{4..256}, p = 2n,
-           m ~ U{0..n/4}, one packed call (size-binned plan)
+           m ~ U{0..n/4}, one packed call (size-binned plan, CUDA graph)
   elastic  1024 elastic QPs (solve_qp_elastic_primal) n = 64, p = 128,
            penalty 1e3, 30% of them infeasible
+`--workload X` runs one of them alone, with its variants.
 
 --impl reference times the FP64 CPU restatement of qpax (oracle/) on the
 host cores, on the same workload -- qpax itself (JAX) is not installable
