@@ -199,7 +199,7 @@ def dist_setup(gpus):
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return world, rank, local
@@ -293,7 +293,7 @@ def run_reference(args, spec: Spec, world, rank):
         "impl": "reference", "metric": metric_for(spec), "value": val, "unit": "QPs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_for(spec, 1),
+        "config": config_for(spec, world),
         "cpu_baseline": {"value": val, "unit": "QPs/s", "cores": cores, "kind": "port",
                          "sample": f"the first {per_step} QPs of the batch per step, {args.steps} steps"},
         "e2e": {"value": val, "unit": "QPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -627,7 +627,9 @@ def run_ours(args, spec: Spec, world, rank, local):
         sampler = ClockSampler(local) if prec == "auto" else None
         tot, fwd_ms, bwd_ms = time_arm(args, arm, stream, flush, world, args.steps, sampler)
         conv, iters, riters = arm.counts()
-        par = arm.parity(data) if (rank == 0 and not args.no_parity) else None
+        # the oracle checks (host work on rank 0 while the other ranks wait at
+        # the next barrier) run in single-GPU runs only
+        par = arm.parity(data) if (world == 1 and not args.no_parity) else None
         pstats = arm.precision_stats() if (prec == "mixed" and hasattr(arm, "precision_stats")) else None
         results[prec] = dict(total_ms=tot, fwd_ms=fwd_ms, bwd_ms=bwd_ms, conv=conv, iters=iters, riters=riters,
                              clocks=sampler.summary() if sampler else None, parity=par, pstats=pstats)
@@ -671,10 +673,10 @@ def run_ours(args, spec: Spec, world, rank, local):
         "metric": metric_for(spec), "value": value, "unit": "QPs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": main_r["total_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_for(spec, world, extra={
-            "precision": prec_desc, "parallelism": f"batch split x{world}",
-            "launch_shapes": "heuristic" if args.no_tune else "autotuned per size bin at setup (untimed)",
-            "l2": "flushed between steps (256 MB write), outside the per-step events"}),
+        "config": config_for(spec, world),
+        "setup": {"precision": prec_desc, "parallelism": f"batch split x{world}",
+                  "launch_shapes": "heuristic" if args.no_tune else "autotuned per size bin at setup (untimed)",
+                  "l2": "flushed between steps (256 MB write), outside the per-step events"},
         "roofline": roof, "gpu_launches": arm_main.launches * args.steps,
         "iterations": {"forward_mean": float(main_r["iters"].mean()), "relax_mean": float(main_r["riters"].mean()),
                        "converged": float(main_r["conv"].mean())},
@@ -691,7 +693,7 @@ def run_ours(args, spec: Spec, world, rank, local):
             if results["mixed"]["pstats"]:
                 line["variants"][VARIANT_NAMES["mixed"]]["precision_stats"] = results["mixed"]["pstats"]
         line["default_over_plain_fp64"] = v["auto"] / v[plain]
-    if rank == 0 and not args.no_parity:
+    if world == 1 and not args.no_parity:
         line["parity"] = {VARIANT_NAMES[k]: r["parity"] for k, r in results.items()}
         line["parity"]["against"] = ("the FP64 oracle (C restatement of qpax) on the same inputs and the same dl/dx, "
                                      "computed after the timed steps; errors relative per instance, "
@@ -710,7 +712,7 @@ def run_ours(args, spec: Spec, world, rank, local):
     del arm_main
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(spec, data)
-    if spec.key == "dense" and not args.no_configs:
+    if spec.key == "dense" and world == 1 and not args.no_configs:  # single-GPU runs
         line["configs"] = run_configs(args, world, rank, dev, stream, flush)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -737,7 +739,7 @@ def run_configs(args, world, rank, dev, stream, flush):
                  "iterations": {"forward_mean": float(iters.mean()), "relax_mean": float(riters.mean()),
                                 "converged": float(conv.mean())},
                  "gpu_launches": arm.launches * steps}
-        if rank == 0 and not args.no_parity:
+        if world == 1 and not args.no_parity:
             entry["parity"] = arm.parity(data)
         if not args.no_e2e:
             sub = argparse.Namespace(**vars(args))

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kWarpKernelThreads, kMinBlocks) group_kernel(c
 // n_pad = 8 only: four instances per warp ran the NNLS batch (n = 5) 1.4x
 // faster than one per warp; at n_pad = 16 two per warp measured no faster.
 KernelFn kernel_group_f64(int NP) {
-  if (NP == 8) return group_kernel<8, 2, 4>;
+  if (NP == 8) return group_kernel<8, 2, 3>;  // 168 registers: 8 % faster than 128 (which spills)
   return nullptr;
 }
 

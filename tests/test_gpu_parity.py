@@ -139,45 +139,45 @@ def test_gradients_configuration3(prec):
 def test_gradients_vs_central_differences_of_relaxed_map():
     """The backward pass differentiates qpax's relaxed solution x_kappa(theta)
     (pdip_relaxed.py:70-103 relax_qp at target_kappa, started from the
-    solve): central differences of that map, computed on the GPU with tight
-    tolerances (solve 1e-10, relax 1e-11, step 1e-5), against the GPU VJP of
-    ||x - 1||^2 on one instance of the n=16, m=4, p=32 configuration.
-    Directions: every q entry, four h and two b entries, an A entry, a
-    diagonal and a symmetric off-diagonal Q pair, two G entries.  Bars:
-    1e-4 * max(1, |grad|) for dQ, dq, dA, db, dh; dG by qpax's formula
-    (diff_qp.py:8-17, D(lam)(dlam x' + lam dx')) differs from the relaxed
-    map's derivative by several percent here, so it is held to the
-    reference's own FD bound, 0.2 relative (test_qp_derivatives.py:52)."""
+    solve): central differences of that map with the configuration's step
+    1e-6, computed on the GPU with tight tolerances (solve 1e-10, relax
+    1e-11), against the GPU VJP of ||x - 1||^2, on four instances of the
+    n=16, m=4, p=32 configuration.  Directions: every q entry, six h, two b
+    and two A entries, a diagonal and a symmetric off-diagonal Q pair.  Bar:
+    1e-5 * max(1, |grad|) (the oracle's own central differences agree to
+    3e-6 here).  dG is not compared with the relaxed map: qpax's formula
+    (diff_qp.py:8-17, D(lam)(dlam x' + lam dx')) is not that map's
+    derivative in G (the oracle's differences disagree with it by up to 5x on
+    these instances); it is held to the oracle's VJP instead
+    (test_gradients_configuration3, tests/test_gpu_configs.py)."""
     import qpax_b200 as qb
 
-    Q, q, A, b, G, h = [np.ascontiguousarray(a[:1]) for a in wl.config3(8)]
+    Q, q, A, b, G, h = [np.ascontiguousarray(a[:4]) for a in wl.config3(8)]
     n = Q.shape[1]
     x0 = np_(qb.solve_qp(Q, q, A, b, G, h, 1e-5)[0])
     dl = wl.loss_grad(x0)
     _, grads, conv, _ = qb.solve_qp_primal_vjp(Q, q, A, b, G, h, dl, 1e-5, 1e-3)
-    assert int(np_(conv).reshape(-1)[0]) == 1
-    grads = [np_(g).reshape(-1) for g in grads]
+    assert (np_(conv) == 1).all()
+    grads = [np_(g) for g in grads]
     # (argument index in Q q A b G h, flat element indices perturbed together)
-    dirs = [(1, [i]) for i in range(n)] + [(5, [r]) for r in range(4)] + [(3, [0]), (3, [1]), (2, [2])] + \
-           [(0, [0]), (0, [2 * n + 5, 5 * n + 2]), (4, [n + 3]), (4, [7 * n])]
-    step = 1e-5
-    batch = [np.repeat(a, 2 * len(dirs), axis=0) for a in (Q, q, A, b, G, h)]
-    for k, (ai, idx) in enumerate(dirs):
-        for sgn, row in ((1.0, 2 * k), (-1.0, 2 * k + 1)):
-            flat = batch[ai][row].reshape(-1)
-            flat[idx] += sgn * step
-    s = qb.solve_qp(*batch, 1e-10)
-    assert np_(s[4]).min() == 1
-    r = qb.relax_qp(*batch, *s[:4], 1e-11, 1e-3)
-    assert np_(r[4]).min() == 1
-    xk = np_(r[0])
-    for k, (ai, idx) in enumerate(dirs):
-        fd = (xk[2 * k] - xk[2 * k + 1]) @ dl.reshape(-1) / (2 * step)
-        g = grads[ai][idx].sum()
-        if ai == 4:
-            assert abs(fd - g) <= 0.2 * abs(fd), ("dG", idx, fd, g)
-        else:
-            assert abs(fd - g) <= 1e-4 * max(1.0, abs(g)), ("QqAbGh"[ai], idx, fd, g)
+    dirs = [(1, [i]) for i in range(n)] + [(5, [r]) for r in range(6)] + [(3, [0]), (3, [1]), (2, [2]), (2, [9])] + \
+           [(0, [0]), (0, [2 * n + 5, 5 * n + 2])]
+    step = 1e-6
+    for inst in range(4):
+        batch = [np.repeat(a[inst:inst + 1], 2 * len(dirs), axis=0) for a in (Q, q, A, b, G, h)]
+        for k, (ai, idx) in enumerate(dirs):
+            for sgn, row in ((1.0, 2 * k), (-1.0, 2 * k + 1)):
+                flat = batch[ai][row].reshape(-1)
+                flat[idx] += sgn * step
+        s = qb.solve_qp(*batch, 1e-10)
+        assert np_(s[4]).min() == 1
+        r = qb.relax_qp(*batch, *s[:4], 1e-11, 1e-3)
+        assert np_(r[4]).min() == 1
+        xk = np_(r[0])
+        for k, (ai, idx) in enumerate(dirs):
+            fd = (xk[2 * k] - xk[2 * k + 1]) @ dl[inst] / (2 * step)
+            g = grads[ai][inst].reshape(-1)[idx].sum()
+            assert abs(fd - g) <= 1e-5 * max(1.0, abs(g)), (inst, "QqAbGh"[ai], idx, fd, g)
 
 
 @pytest.mark.parametrize("prec", PRECS)
