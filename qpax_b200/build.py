@@ -32,6 +32,7 @@ SOURCES = [
     "qpb_kern_elastic_f64.cu",
     "qpb_kern_elastic_mixed.cu",
     "qpb_kern_warp.cu",
+    "qpb_kern_warp_mixed.cu",
     "qpb_noalloc.cu",
     "qpb_plan.cu",
     "qpb_host_pipeline.cu",

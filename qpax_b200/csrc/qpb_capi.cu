@@ -175,17 +175,20 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl, const 
   const DevInfo di = dev_info();
   if (!di.ok) return QPB_ERR_CUDA;
   pl->gstage_rows = 0;
+  pl->fn_resume = nullptr;
+  pl->hlist_off = pl->hstate_off = pl->hiter_off = 0;
+  pl->hstride = 0;
   const size_t smem_budget = (size_t)di.smem_optin - 1024;  // room for static shared + reserve
   const int np = warp_np(d);
   const int want_threads = ch && ch->team_threads ? ch->team_threads : cfg.team_threads;
   const int cap = ch ? ch->per_sm_cap : 0;
-  if (!elastic && !mixed && np && (want_threads == 0 || want_threads == 32)) {
-    // one warp per instance (n_pad = 16, 32) or four instances per warp in
-    // lockstep (n_pad = 8), FP64, four warps per CTA; `teams` counts
-    // instances per CTA
-    KernelFn gfn = kernel_group_f64(np);
+  if (!elastic && np && (want_threads == 0 || want_threads == 32)) {
+    // one warp per instance (n_pad = 16, 32; mixed precision at every
+    // n_pad) or four instances per warp in lockstep (n_pad = 8, FP64), four
+    // warps per CTA; `teams` counts instances per CTA
+    KernelFn gfn = mixed ? nullptr : kernel_group_f64(np);
     const int per_warp = gfn ? 32 / np : 1;
-    KernelFn fn = gfn ? gfn : kernel_warp_f64(np);
+    KernelFn fn = gfn ? gfn : (mixed ? kernel_warp_mixed(np) : kernel_warp_f64(np));
     if (!fn) return QPB_ERR_UNSUPPORTED;
     size_t arena = (WarpArena::bytes(np, np / 4, d.p) + 255) & ~size_t(255);
     pl->fn = (const void*)fn;
@@ -212,6 +215,21 @@ int make_plan(int op, const qpb_dims& d, const qpb_config& cfg, Plan* pl, const 
     grid = grid > need ? need : grid;
     pl->grid = (int)(grid < 1 ? 1 : grid);
     pl->ws_bytes = kCounterBytes + (pl->in_smem ? 0 : (size_t)pl->grid * pl->teams * arena);
+    if (mixed) {
+      // instances whose FP32 factor is rejected continue on the FP64 kernel
+      // (same arena layout), from their iterate in the hand-over region
+      pl->fn_resume = (const void*)kernel_warp_f64(np);
+      if (!pl->fn_resume) return QPB_ERR_UNSUPPORTED;
+      int v = 0;  // (also raises the resume kernel's dynamic shared-memory limit)
+      if (occupancy(pl->fn_resume, pl->threads, pl->smem_bytes, &v) != QPB_OK) return QPB_ERR_CUDA;
+      if (v < 1) return QPB_ERR_UNSUPPORTED;
+      const size_t B = (size_t)d.batch;
+      pl->hstride = d.n + 2 * d.p + d.m;
+      pl->hlist_off = (pl->ws_bytes + 255) & ~size_t(255);
+      pl->hstate_off = pl->hlist_off + ((4 * B + 255) & ~size_t(255));
+      pl->hiter_off = pl->hstate_off + ((12 * B + 255) & ~size_t(255));
+      pl->ws_bytes = pl->hiter_off + 8 * B * (size_t)pl->hstride;
+    }
     return QPB_OK;
   }
   const int KC = chunks_for(d.n > d.m ? d.n : d.m);
@@ -305,7 +323,7 @@ static std::vector<LaunchChoice> tune_candidates(int op, const qpb_dims& d, cons
   const bool mixed = c.precision == QPB_PRECISION_MIXED;
   const int KC = chunks_for(d.n > d.m ? d.n : d.m);
   std::vector<int> teams;
-  if ((!elastic && !mixed && warp_np(d)) || KC == 1) teams.push_back(32);
+  if ((!elastic && warp_np(d)) || KC == 1) teams.push_back(32);
   teams.push_back(128);
   if (KC >= 4) teams.push_back(256);
   const int sms = device_sms();
@@ -367,18 +385,11 @@ int tune_pick(Params P, int op, const qpb_dims& d, const qpb_config& cfg, void* 
     if (sample > d.batch) sample = d.batch;
     Params R = P;
     R.batch = (int)sample;
-    R.counter = reinterpret_cast<int*>(ws);
-    R.arena = reinterpret_cast<unsigned char*>(ws) + kCounterBytes;
-    R.arena_bytes = pl.arena_bytes;
-    R.arena_in_smem = pl.in_smem;
-    R.gstage_rows = pl.gstage_rows;
     const long need_teams = (sample + pl.teams - 1) / pl.teams;
     const int grid = (int)(need_teams < pl.grid ? need_teams : pl.grid);
     float ms = 0.0f;
     for (int rep = 0; rep < 2 && status == QPB_OK; ++rep) {  // the first run warms the caches
-      void* args[] = {&R};
-      if (cudaMemsetAsync(ws, 0, sizeof(int), st) != cudaSuccess || cudaEventRecord(e0, st) != cudaSuccess ||
-          cudaLaunchKernel(pl.fn, dim3(grid), dim3(pl.threads), args, pl.smem_bytes, st) != cudaSuccess ||
+      if (cudaEventRecord(e0, st) != cudaSuccess || enqueue(pl, R, ws, grid, st) != QPB_OK ||
           cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
           cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
         status = QPB_ERR_CUDA;
@@ -461,16 +472,38 @@ static int launch(Params P, const qpb_dims* d, const qpb_config* cfg, void* ws, 
   P.pivot_max = c.pivot_max;
   P.max_sweeps = c.max_sweeps;
   P.stats = c.stats;
-  P.counter = reinterpret_cast<int*>(ws);
-  P.arena = reinterpret_cast<unsigned char*>(ws) + kCounterBytes;
+  return enqueue(pl, P, ws, pl.grid, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int enqueue(const Plan& pl, Params P, void* ws, int grid, cudaStream_t s) {
+  unsigned char* w = reinterpret_cast<unsigned char*>(ws);
+  int* ctr = reinterpret_cast<int*>(ws);  // [0] work counter, [2] resume counter, [4] hand-overs
+  P.counter = ctr;
+  P.arena = w + kCounterBytes;
   P.arena_bytes = pl.arena_bytes;
   P.arena_in_smem = pl.in_smem;
   P.gstage_rows = pl.gstage_rows;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (cudaMemsetAsync(ws, 0, sizeof(int), s) != cudaSuccess) return QPB_ERR_CUDA;
+  P.resume = 0;
+  if (pl.fn_resume) {
+    P.hcount = ctr + 4;
+    P.hlist = reinterpret_cast<int32_t*>(w + pl.hlist_off);
+    P.hstate = reinterpret_cast<int32_t*>(w + pl.hstate_off);
+    P.hiter = reinterpret_cast<double*>(w + pl.hiter_off);
+    P.hstride = pl.hstride;
+  }
+  if (cudaMemsetAsync(ws, 0, 64, s) != cudaSuccess) return QPB_ERR_CUDA;
   void* args[] = {&P};
-  if (cudaLaunchKernel(pl.fn, dim3(pl.grid), dim3(pl.threads), args, pl.smem_bytes, s) != cudaSuccess)
+  if (cudaLaunchKernel(pl.fn, dim3(grid), dim3(pl.threads), args, pl.smem_bytes, s) != cudaSuccess)
     return QPB_ERR_CUDA;
+  if (pl.fn_resume) {
+    Params R = P;
+    R.resume = 1;
+    R.mixed = 0;
+    R.counter = ctr + 2;
+    void* rargs[] = {&R};
+    if (cudaLaunchKernel(pl.fn_resume, dim3(grid), dim3(pl.threads), rargs, pl.smem_bytes, s) != cudaSuccess)
+      return QPB_ERR_CUDA;
+  }
   return QPB_OK;
 }
 

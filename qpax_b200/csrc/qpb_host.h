@@ -4,6 +4,8 @@
 #include <stddef.h>
 
 #include "../../include/qpb.h"
+#include <cuda_runtime_api.h>
+
 #include "qpb_params.h"
 
 namespace qpb {
@@ -18,7 +20,19 @@ struct Plan {
   size_t arena_bytes, smem_bytes, ws_bytes;
   int in_smem;
   int gstage_rows;  // rows of G per shared-memory chunk (arena in global memory), 0: none
+  // mixed precision on the one-warp kernels: the FP64 kernel that resumes
+  // the instances the mixed launch hands over (nullptr: one launch), and
+  // the hand-over region of the workspace (list, states, iterate blocks)
+  const void* fn_resume;
+  size_t hlist_off, hstate_off, hiter_off;
+  int hstride;
 };
+
+// Enqueues the plan's launch(es) on `s`: zeroes the work counters, runs the
+// persistent kernel over P.batch instances with `grid` CTAs and, for
+// mixed-precision warp plans, the FP64 resume launch after it.  Sets P's
+// counter, arena and hand-over fields from `ws`.
+int enqueue(const Plan& pl, Params P, void* ws, int grid, cudaStream_t s);
 
 // A launch shape chosen by the autotuner (zero fields: the heuristic's choice).
 struct LaunchChoice {

@@ -55,6 +55,18 @@ struct Params {
   const int32_t *shapes;
   const int64_t *offs;
   const int32_t *list;
+  // Mixed precision on the one-warp kernels runs in two launches: the mixed
+  // kernel hands an instance whose FP32 factor is rejected (pivot ratio,
+  // refinement stall) over to the FP64 kernel, which resumes it where it
+  // stopped.  Per launch-local instance index li: iterate block
+  // hiter[li * hstride ...] = x (n) | s (p) | z (p) | y (m), with the
+  // launch's (largest) n, m, p; hstate[3 li ...] = stage, iteration,
+  // converged; hlist[0 .. *hcount) = the handed-over indices.
+  int resume;           // 1: this launch resumes the instances in hlist (FP64 kernel)
+  int *hcount;
+  int32_t *hlist, *hstate;
+  double *hiter;
+  int hstride;
 };
 
 // Where instance `inst` (a launch-local index) lives.

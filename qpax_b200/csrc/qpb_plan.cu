@@ -59,9 +59,8 @@ static void free_plan(qpb_plan* pl) {
 
 // Bin key: the kernel variant an instance runs on.
 static int bin_key(const qpb_dims& d, const qpb_config& c) {
-  const bool mixed = c.precision == QPB_PRECISION_MIXED;
   const int np = warp_np(d);
-  if (!mixed && np && (c.team_threads == 0 || c.team_threads == 32)) return np;  // 8, 16, 32
+  if (np && (c.team_threads == 0 || c.team_threads == 32)) return np;  // 8, 16, 32 (FP64 or mixed)
   const int kc = chunks_for(d.n > d.m ? d.n : d.m);
   return 1000 + kc;  // team kernel, KC register chunks
 }
@@ -242,16 +241,8 @@ static int launch_packed(const qpb_plan* pl, Params P, void* ws, size_t ws_bytes
     Q.m = b.m_max;
     Q.p = b.p_max;
     Q.list = pl->d_list + b.list_off;
-    Q.counter = reinterpret_cast<int*>(wsb);
-    Q.arena = wsb + kCounterBytes;
-    Q.arena_bytes = b.launch.arena_bytes;
-    Q.arena_in_smem = b.launch.in_smem;
-    Q.gstage_rows = b.launch.gstage_rows;
-    if (cudaMemsetAsync(wsb, 0, sizeof(int), s) != cudaSuccess) return QPB_ERR_CUDA;
-    void* args[] = {&Q};
-    if (cudaLaunchKernel(b.launch.fn, dim3(b.launch.grid), dim3(b.launch.threads), args, b.launch.smem_bytes, s) !=
-        cudaSuccess)
-      return QPB_ERR_CUDA;
+    const int st = enqueue(b.launch, Q, wsb, b.launch.grid, s);
+    if (st != QPB_OK) return st;
     if (k > 0) {
       if (cudaEventRecord(pl->events[k], s) != cudaSuccess) return QPB_ERR_CUDA;
       if (cudaStreamWaitEvent(s0, pl->events[k], 0) != cudaSuccess) return QPB_ERR_CUDA;

@@ -57,6 +57,12 @@ struct WarpArena {
   static size_t bytes(int NP, int MP, int p) { return doubles(NP, MP, p) * sizeof(double) + 16; }
 };
 
+// Starting iterate of one instance: the caller's arrays, or the block a
+// mixed-kernel hand-over left in the workspace.
+struct IterSrc {
+  const double *x, *s, *z, *y;
+};
+
 enum WarpSlot : int { kVh = 0, kVs, kVz, kVw, kVv2, kVv3, kVds, kVdz, kVtp };
 
 template <int NP, int MP>
@@ -82,10 +88,12 @@ struct WarpAddr {
   QPB_DEV double* F() const { return Y() + (MP > 8 ? MP : 8) * (NP + 1); }
 };
 
-template <int NP, int MP>
+// kMixed: FP32 factorisation with FP64 iterative refinement (the mixed
+// precision mode); the FP64 instantiation is unaffected by it.
+template <int NP, int MP, bool kMixed = false>
 struct WarpQP {
   static_assert(NP == 8 || NP == 16 || NP == 32, "NP");
-  static constexpr int kYld = NP + 1;  // row stride of Y
+  static constexpr int kYld = NP + 1;  // row stride of Y (doubles, or floats in the FP32 factor)
   // Column swizzle of G's row r (period 4 in r): the four rows of one DMMA
   // k-step fall in distinct shared-memory banks.
   static QPB_DEV int gswz(int r) { return NP == 8 ? (r & 2) << 1 : (4 * r) & 12; }
@@ -102,6 +110,14 @@ struct WarpQP {
   double x, q;       // n-vectors (lane j)
   double y, b;       // m-vectors (lane i)
   int st_f64, st_flags;
+  // mixed precision: hc[] keeps H in FP64 (the refinement's operator) and
+  // lf[] holds the FP32 factor (lane-owned column); its D^-1, Y, F live in
+  // the FP64 factor's shared regions.
+  float lf[NP];
+  int st_f32, st_sweeps;
+  float dinvf, fdinvf;
+  double pivot_max;
+  int max_sweeps;
 
   QPB_DEV void setup(const Params& prm, unsigned char* arena, int ln) {
     P = &prm;
@@ -109,7 +125,12 @@ struct WarpQP {
     lane = ln;
     a.base = reinterpret_cast<double*>(arena);
     a.p = p;
+    if constexpr (kMixed) {
+      pivot_max = prm.pivot_max;
+      max_sweeps = prm.max_sweeps;
+    }
   }
+
 
   // qv[i] = sym(Q)[i][lane]: (Q + Q')/2, or the coalesced Q[i][lane] alone
   // when Q is exactly symmetric (checked once per instance).  All loads are
@@ -137,8 +158,9 @@ struct WarpQP {
   // arena.  A shared-memory arena is filled with asynchronous copies, every
   // row in flight at once (one memory round trip per instance); a global
   // arena (large p) with grouped loads.  Rows with h = inf are zeroed in G and
-  // h when remove_inf (qpax/pdip.py:166-178).
-  QPB_DEV void load(const InstRef& R, bool remove_inf, bool iterate) {
+  // h when remove_inf (qpax/pdip.py:166-178).  `it` points at the starting
+  // iterate (x, s, z, y) of this instance.
+  QPB_DEV void load(const InstRef& R, bool remove_inf, bool iterate, const IterSrc& it) {
     gQ = P->Q + R.oQ;
     const double* gG = P->G + R.oG;
     const double* gA = P->A + R.oA;
@@ -160,8 +182,8 @@ struct WarpQP {
       for (int r = lane; r < p; r += 32) cp_async8(a.h() + r, gh + r);
       if (iterate) {
         for (int r = lane; r < p; r += 32) {
-          cp_async8(a.s() + r, P->in[1] + R.oh + r);
-          cp_async8(a.z() + r, P->in[2] + R.oh + r);
+          cp_async8(a.s() + r, it.s + r);
+          cp_async8(a.z() + r, it.z + r);
         }
       }
       cp_async_wait_all();
@@ -203,16 +225,16 @@ struct WarpQP {
       }
       if (iterate) {
         for (int r = lane; r < p; r += 32) {
-          a.s()[r] = P->in[1][R.oh + r];
-          a.z()[r] = P->in[2][R.oh + r];
+          a.s()[r] = it.s[r];
+          a.z()[r] = it.z[r];
         }
       }
     }
     q = (lane < n) ? P->q[R.oq + lane] : 0.0;
     b = (lane < m) ? P->b[R.ob + lane] : 0.0;
     if (iterate) {
-      x = (lane < n) ? P->in[0][R.oq + lane] : 0.0;
-      y = (lane < m) ? P->in[3][R.ob + lane] : 0.0;
+      x = (lane < n) ? it.x[lane] : 0.0;
+      y = (lane < m) ? it.y[lane] : 0.0;
     }
     int asym = 0;
 #pragma unroll
@@ -333,22 +355,160 @@ struct WarpQP {
 
 
   // ---------------------------------------------------------------- factor
-  // H = sym(Q) + G' diag(w) G (w in shared memory), LDL^T in registers,
-  // then Y = L^-1 A' and F = Y D^-1 Y' with its LDL^T in shared memory.
-  QPB_DEV void factor() {
-    st_f64++;
-    dinv = 0.0;
-    fdinv = 0.0;
+  // Factor for the weights in shared memory: FP64, or (mixed) FP32.
+  // Returns false when the mixed kernel's FP32 factor is rejected: the
+  // instance is then handed over to the FP64 kernel (the mixed kernel holds
+  // no FP64 factorisation, which keeps its code within the instruction
+  // cache: both fully unrolled eliminations in one kernel thrash it).
+  QPB_DEV bool factor() {
+    if constexpr (kMixed) {
+      form_hfull();
+      if (ldlt32()) {
+        st_f32++;
+        return true;
+      }
+      st_flags |= kFlagFallback;
+      return false;
+    } else {
+      factor64();
+      return true;
+    }
+  }
+
+  // hc = column `lane` of H = sym(Q) + G' diag(w) G in FP64 (identity
+  // columns beyond n)
+  QPB_DEV void form_hfull() {
     // (starting from zeros rather than from Q keeps hc in registers)
 #pragma unroll
     for (int i = 0; i < NP; ++i) hc[i] = 0.0;
     form_h_tensor();
-    {
-      double qv[NP];
-      load_q(qv);
+    double qv[NP];
+    load_q(qv);
 #pragma unroll
-      for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qv[i] + hc[i];
+    for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qv[i] + hc[i];
+  }
+
+  // Mixed: H (FP64 in hc, from form_hfull, kept there) rounded to FP32 and
+  // factored in FP32 in lf[]; Y = L^-1 A' in the same loop, F = Y' D^-1 Y
+  // from the FP32 Y with FP64 products, and F's LDL^T, all in FP32.
+  // Returns false when a pivot is not positive and finite or the pivot
+  // ratio max(d)/min(d) of H exceeds pivot_max.
+  QPB_DEV bool ldlt32() {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) lf[i] = __double2float_rn(hc[i]);
+    int bad = 0;
+    float dmax = 0.0f, dmin = INFINITY;
+    float* cb = reinterpret_cast<float*>(a.cb());
+    float* yb = reinterpret_cast<float*>(a.Y());
+    float yc[MP];
+#pragma unroll
+    for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? __double2float_rn(a.A()[i * NP + lane]) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      if (lane < NP) cb[lane] = lf[k];
+      if (lane == k) {
+#pragma unroll
+        for (int i = 0; i < MP; ++i) yb[i] = yc[i];
+      }
+      __syncwarp();
+      const float dk = cb[k];
+      const float rk = __frcp_rn(dk);
+      if (k < n) {
+        bad |= !(dk > 0.0f) || !isfinite(dk);
+        dmax = fmaxf(dmax, dk);
+        dmin = fminf(dmin, dk);
+      }
+      if (lane == k) dinvf = rk;
+      const float hk = lf[k];
+      if (lane > k) {
+        if ((k + 1) & 1) lf[k + 1] = fmaf(-(cb[k + 1] * hk), rk, lf[k + 1]);
+#pragma unroll
+        for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
+          const float2 c2 = *reinterpret_cast<const float2*>(cb + i2);
+          lf[i2] = fmaf(-(c2.x * hk), rk, lf[i2]);
+          lf[i2 + 1] = fmaf(-(c2.y * hk), rk, lf[i2 + 1]);
+        }
+        const float l = hk * rk;
+#pragma unroll
+        for (int i = 0; i < MP; ++i) yc[i] = fmaf(-l, yb[i], yc[i]);
+      }
+      __syncwarp();
     }
+    float* dvf = reinterpret_cast<float*>(a.dvi());
+    float* Yf = reinterpret_cast<float*>(a.Y());
+    if (lane < NP) {
+      dvf[lane] = dinvf;
+#pragma unroll
+      for (int i = 0; i < MP; ++i) Yf[i * kYld + lane] = yc[i];
+    }
+    __syncwarp();
+    // F = Y' D^-1 Y: products of FP32 values are exact in FP64 (one DMMA
+    // tile, as factor64), the sum rounded to FP32
+    float* Ff = reinterpret_cast<float*>(a.F());
+    {
+      const int g = lane >> 2, t = lane & 3;
+      double f0 = 0.0, f1 = 0.0;
+#pragma unroll
+      for (int kb = 0; kb < NP / 4; ++kb) {
+        const int j = 4 * kb + t;
+        const double b0 = (g < MP) ? (double)Yf[g * kYld + j] : 0.0;
+        dmma884(f0, f1, b0 * (double)dvf[j], b0);
+      }
+      __syncwarp();
+      if (g < MP) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int c = 2 * t + u;
+          if (c < MP) Ff[g * MP + c] = (g < m && c < m) ? __double2float_rn(u ? f1 : f0) : (g == c ? 1.0f : 0.0f);
+        }
+      }
+    }
+    __syncwarp();
+    fdinvf = 0.0f;
+    {
+      float fc[MP];
+#pragma unroll
+      for (int i = 0; i < MP; ++i) fc[i] = (lane < MP) ? Ff[i * MP + lane] : 0.0f;
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < MP; ++k) {
+        if (lane == k) {
+#pragma unroll
+          for (int i = 0; i < MP; ++i) cb[i] = fc[i];
+        }
+        __syncwarp();
+        const float dk = cb[k];
+        const float rk = __frcp_rn(dk);
+        if (k < m) bad |= !(dk > 0.0f) || !isfinite(dk);
+        if (lane == k) fdinvf = rk;
+        if (lane > k && lane < MP) {
+          const float f = fc[k] * rk;
+#pragma unroll
+          for (int i = k + 1; i < MP; ++i) fc[i] = fmaf(-cb[i], f, fc[i]);
+        }
+        __syncwarp();
+      }
+      if (lane < MP) {
+#pragma unroll
+        for (int i = 0; i < MP; ++i) Ff[i * MP + lane] = fc[i];
+      }
+      __syncwarp();
+    }
+    return !bad && (double)dmax <= pivot_max * (double)dmin;
+  }
+
+  // H = sym(Q) + G' diag(w) G (w in shared memory), LDL^T in registers,
+  // then Y = L^-1 A' and F = Y D^-1 Y' with its LDL^T in shared memory.
+  QPB_DEV void factor64() {
+    form_hfull();
+    ldlt64();
+  }
+
+  // LDL^T of H (in hc) in FP64, then Y, F and F's factor.
+  QPB_DEV void ldlt64() {
+    st_f64++;
+    dinv = 0.0;
+    fdinv = 0.0;
     // LDL^T: step k broadcasts row k of the Schur complement (= column k);
     // Y = L^-1 A' is formed in the same loop: lane j holds Y[j][0..MP), and
     // step k broadcasts lane k's (final) row of Y beside the pivot row.
@@ -456,8 +616,135 @@ struct WarpQP {
   QPB_DEV double fcol(int k) const { return lane < MP ? a.F()[k * MP + lane] : 0.0; }
 
   // --------------------------------------------------------- reduced solve
-  // [H A'; A 0][dx; dy] = [r; v]  (r lane j < n, v lane i < m)
-  QPB_DEV void reduced(double r, double v, double& odx, double& ody) {
+  // [H A'; A 0][dx; dy] = [r; v]  (r lane j < n, v lane i < m).  Returns
+  // false only in the mixed kernel, when FP64 refinement against the FP32
+  // factor stalls (the instance is handed over to the FP64 kernel).
+  QPB_DEV bool reduced(double r, double v, double& odx, double& ody) {
+    if constexpr (kMixed) {
+      if (reduced_refined(r, v, odx, ody)) return true;
+      st_flags |= kFlagRefineStall | kFlagFallback;
+      return false;
+    } else {
+      reduced64(r, v, odx, ody);
+      return true;
+    }
+  }
+
+  static QPB_DEV float wmaxf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+  }
+  static QPB_DEV float wsumf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+  }
+
+  // As reduced64, in FP32 with the FP32 factor.
+  QPB_DEV void reduced32(float r, float v, float& odx, float& ody) const {
+    const float* dvf = reinterpret_cast<const float*>(a.dvi());
+    const float* Yf = reinterpret_cast<const float*>(a.Y());
+    const float* Ff = reinterpret_cast<const float*>(a.F());
+    float u = (lane < n) ? r : 0.0f;
+#pragma unroll
+    for (int k = 0; k < NP - 1; ++k) {
+      const float uk = __shfl_sync(kFull, u, k) * dvf[k];
+      if (lane > k) u = fmaf(-lf[k], uk, u);
+    }
+    const float ud = (lane < NP) ? u * dinvf : 0.0f;
+    float g = 0.0f;
+#pragma unroll
+    for (int i = 0; i < MP; ++i) {
+      const float gi = wsumf((lane < NP ? Yf[i * kYld + lane] : 0.0f) * ud);
+      if (lane == i) g = gi - v;
+    }
+    if (lane >= m) g = 0.0f;
+#pragma unroll
+    for (int k = 0; k < MP - 1; ++k) {
+      const float gk = __shfl_sync(kFull, g, k) * __shfl_sync(kFull, fdinvf, k);
+      if (lane > k && lane < MP) g = fmaf(-Ff[k * MP + lane], gk, g);
+    }
+    g = (lane < MP) ? g * fdinvf : 0.0f;
+#pragma unroll
+    for (int k = MP - 1; k > 0; --k) {
+      const float gk = __shfl_sync(kFull, g, k);
+      if (lane < k) g = fmaf(-Ff[k * MP + lane] * fdinvf, gk, g);
+    }
+    ody = (lane < m) ? g : 0.0f;
+    float wv = u;
+#pragma unroll
+    for (int i = 0; i < MP; ++i) wv = fmaf(-(lane < NP ? Yf[i * kYld + lane] : 0.0f), __shfl_sync(kFull, g, i), wv);
+    float xv = (lane < NP) ? wv * dinvf : 0.0f;
+#pragma unroll
+    for (int k = NP - 1; k > 0; --k) {
+      const float xk = __shfl_sync(kFull, xv, k);
+      if (lane < k) xv = fmaf(-lf[k] * dinvf, xk, xv);
+    }
+    odx = (lane < n) ? xv : 0.0f;
+  }
+
+  // Mixed: FP32 solves with FP64 iterative refinement against the FP64
+  // operator [H, A'; A, 0], H = sym(Q) + G' diag(w) G as formed in FP64 for
+  // this factor (hc: lane j holds column j, so (H dx)_j is one 32-term dot
+  // product per lane).  Sweep 0 solves for the right-hand side itself; each
+  // later sweep solves for the residual of the current solution and adds
+  // the correction.  Stops when the correction, or the next one predicted
+  // from the observed contraction, is below 1e-12 of the solution; returns
+  // false when the corrections stop shrinking or max_sweeps refinement
+  // sweeps do not get there.
+  QPB_DEV bool reduced_refined(double r, double v, double& odx, double& ody) {
+    double dx = 0.0, dy = 0.0, prev = INFINITY;
+    double rx = (lane < n) ? r : 0.0, ry = (lane < m) ? v : 0.0;
+#pragma unroll 1
+    for (int sw = 0; sw <= max_sweeps; ++sw) {
+      if (sw > 0) {
+        if (lane < NP) a.xs()[lane] = dx;
+        __syncwarp();
+        const double* xsv = a.xs();
+        double h0 = 0.0, h1 = 0.0;
+#pragma unroll
+        for (int i = 0; i < NP; i += 2) {
+          const double2 x2 = *reinterpret_cast<const double2*>(xsv + i);
+          h0 = fma(hc[i], x2.x, h0);
+          h1 = fma(hc[i + 1], x2.y, h1);
+        }
+        double ad = 0.0, adx = 0.0;
+#pragma unroll
+        for (int i = 0; i < MP; ++i) {
+          ad = fma(ycol_a(i), __shfl_sync(kFull, dy, i), ad);
+          const double s = wsum(ycol_a(i) * dx);
+          if (lane == i) adx = s;
+        }
+        rx = (lane < n) ? r - ((h0 + h1) + ad) : 0.0;
+        ry = (lane < m) ? v - adx : 0.0;
+        __syncwarp();  // xs read before it is written again
+      }
+      float ex, ey;
+      reduced32(__double2float_rn(rx), __double2float_rn(ry), ex, ey);
+      dx += (double)ex;
+      dy += (double)ey;
+      if (sw > 0) {
+        st_sweeps++;
+        // |correction| / |solution| over (dx, dy) jointly; a ratio test
+        // needs no more than FP32
+        const float en = wmaxf(fmaxf(fabsf(ex), fabsf(ey)));
+        const float dn = wmaxf(fmaxf(__double2float_rn(fabs(dx)), __double2float_rn(fabs(dy))));
+        const double rel = (double)en / (dn > 0.0f ? (double)dn : 1.0);
+        if (rel <= 1e-12 || (sw > 1 && rel * (rel / prev) <= 1e-12)) {
+          odx = dx;
+          ody = dy;
+          return true;
+        }
+        if (!(rel < 0.5 * prev)) return false;
+        prev = rel;
+      }
+    }
+    return false;
+  }
+
+  // FP64 factor: [H A'; A 0][dx; dy] = [r; v]  (r lane j < n, v lane i < m)
+  QPB_DEV void reduced64(double r, double v, double& odx, double& ody) {
     double u = (lane < n) ? r : 0.0;  // u = L^-1 r
 #pragma unroll
     for (int k = 0; k < NP - 1; ++k) {
@@ -540,7 +827,8 @@ struct WarpQP {
   // ------------------------------------------------------------ KKT solve
   // qpax/pdip.py:49-63.  With slack == false the right-hand side is the
   // reduced one directly ([H A'; A 0][dx; dy] = [c1; c4], qpax/pdip.py:22-24).
-  QPB_DEV void solve(bool slack, double c1, const double* c2, const double* c3, double c4, double& odx,
+  // Returns false when the mixed mode's refinement stalled (nothing written).
+  QPB_DEV bool solve(bool slack, double c1, const double* c2, const double* c3, double c4, double& odx,
                      double& ody) {
     double p1 = c1;
     if (slack) {
@@ -549,7 +837,7 @@ struct WarpQP {
       __syncwarp();
       p1 = (lane < n) ? c1 + gcol_dot(tp) : 0.0;
     }
-    reduced(p1, c4, odx, ody);
+    if (!reduced(p1, c4, odx, ody)) return false;
     if (slack) {
       if (lane < NP) a.xs()[lane] = odx;
       __syncwarp();
@@ -562,6 +850,7 @@ struct WarpQP {
       }
       __syncwarp();
     }
+    return true;
   }
 
   // -(relaxed KKT residuals): v1, v4 returned in registers, v2, v3 and
@@ -644,9 +933,40 @@ struct WarpQP {
   // --------------------------------------------------------------- driver
   enum Stage : int { kInit, kStep, kCorrector, kAdjoint, kDone };
 
+  // Mixed kernel: hands this instance over to the FP64 kernel, to resume
+  // at `stage` from the current iterate with `it` iterations done and the
+  // converged flag so far; records what the mixed kernel did in `stats`.
+  QPB_DEV void hand_over(const InstRef& R, long li, int stage, int it, int converged) {
+    double* hb = P->hiter + li * (long)P->hstride;
+    if (lane < n) hb[lane] = x;
+    for (int r = lane; r < p; r += 32) {
+      hb[P->n + r] = a.s()[r];
+      hb[P->n + P->p + r] = a.z()[r];
+    }
+    if (lane < m) hb[P->n + 2 * P->p + lane] = y;
+    if (lane == 0) {
+      P->hstate[3 * li] = stage;
+      P->hstate[3 * li + 1] = it;
+      P->hstate[3 * li + 2] = converged;
+      P->hlist[atomicAdd(P->hcount, 1)] = (int32_t)li;
+      if (P->stats) {
+        P->stats[R.id * 4 + kStatFact32] = st_f32;
+        P->stats[R.id * 4 + kStatFact64] = 0;
+        P->stats[R.id * 4 + kStatSweeps] = st_sweeps;
+        P->stats[R.id * 4 + kStatFlags] = st_flags;
+      }
+    }
+    __syncwarp();
+  }
+
+  // Instance i of this launch; a resume launch (FP64 kernel after the
+  // mixed one) takes the i-th handed-over instance.
   QPB_DEV void run(long i) {
     st_f64 = st_flags = 0;
-    const InstRef R = inst_ref(*P, i);
+    if constexpr (kMixed) st_f32 = st_sweeps = 0;
+    const bool resume = !kMixed && P->resume;
+    const long li = resume ? (long)P->hlist[i] : i;  // launch-local index
+    const InstRef R = inst_ref(*P, li);
     n = R.n;
     m = R.m;
     p = R.p;
@@ -655,7 +975,6 @@ struct WarpQP {
     const int op = P->op;
     const bool relaxed = (op == kOpRelax || op == kOpBwd);
     const bool fresh = (op == kOpSolve || op == kOpInit);
-    load(R, op == kOpSolve, !fresh);
     int stage;
     if (fresh)
       stage = kInit;
@@ -663,6 +982,18 @@ struct WarpQP {
       stage = (op == kOpAdjoint) ? kAdjoint : kStep;
     if (op == kOpSolve && p == 0) stage = kInit;
     int it = 0, converged = 0, conv_now = 0;
+    IterSrc src{nullptr, nullptr, nullptr, nullptr};
+    if (!fresh) src = IterSrc{P->in[0] + R.oq, P->in[1] + R.oh, P->in[2] + R.oh, P->in[3] + R.ob};
+    bool from_iterate = !fresh;
+    if (resume) {
+      stage = P->hstate[3 * li];
+      it = P->hstate[3 * li + 1];
+      converged = P->hstate[3 * li + 2];
+      const double* hb = P->hiter + li * (long)P->hstride;
+      src = IterSrc{hb, hb + P->n, hb + P->n + P->p, hb + P->n + 2 * P->p};
+      from_iterate = stage != kInit;
+    }
+    load(R, op == kOpSolve, from_iterate, src);
     double v1 = 0.0, v4 = 0.0, dxr = 0.0, dyr = 0.0;
     double sigma_mu = 0.0;
     // bounded: initial point + 2 solves per iteration + adjoint
@@ -704,8 +1035,17 @@ struct WarpQP {
         c1 = (lane < n) ? -P->gx[R.oq + lane] : 0.0;
         c3 = a.v2();
       }
-      if (refactor) factor();
-      solve(slack, c1, c2, c3, c4, dxr, dyr);
+      if constexpr (kMixed) {
+        // FP32 factor rejected or refinement stalled: the FP64 kernel takes
+        // over (a corrector restarts its iteration from the residuals)
+        if ((refactor && !factor()) || !solve(slack, c1, c2, c3, c4, dxr, dyr)) {
+          hand_over(R, li, stage == kCorrector ? (int)kStep : stage, it, converged);
+          return;
+        }
+      } else {
+        if (refactor) factor();
+        solve(slack, c1, c2, c3, c4, dxr, dyr);
+      }
       // ---- consume the solution
       if (stage == kInit) {
         x = dxr;
@@ -770,10 +1110,13 @@ struct WarpQP {
     if (lane == 0) {
       if (P->conv) P->conv[inst] = (op == kOpInit || op == kOpAdjoint) ? 0 : converged;
       if (P->iters) P->iters[inst] = it;
-      if (P->stats) {
-        P->stats[inst * 4 + kStatFact32] = 0;
+      if (P->stats && resume) {  // added to the mixed kernel's record
+        P->stats[inst * 4 + kStatFact64] += st_f64;
+        P->stats[inst * 4 + kStatFlags] |= st_flags;
+      } else if (P->stats) {
+        P->stats[inst * 4 + kStatFact32] = kMixed ? st_f32 : 0;
         P->stats[inst * 4 + kStatFact64] = st_f64;
-        P->stats[inst * 4 + kStatSweeps] = 0;
+        P->stats[inst * 4 + kStatSweeps] = kMixed ? st_sweeps : 0;
         P->stats[inst * 4 + kStatFlags] = st_flags;
       }
     }

@@ -10,7 +10,8 @@ for each kernel family:
   "auto":     the default dispatch (one warp per instance in FP64 for n <= 32, m <= n_pad/4,
               one CTA per instance in FP64 above)
   "fp64-cta": one CTA per instance, FP64 factor (the plain FP64 kernel)
-  "mixed":    one CTA per instance, FP32 factor + FP64 refinement + FP64 fallback
+  "mixed":    FP32 factor + FP64 refinement + FP64 fallback (one warp per instance for
+              n <= 32, m <= n_pad/4, one CTA per instance above)
 """
 
 import numpy as np
