@@ -111,9 +111,9 @@ struct WarpQP {
   double y, b;       // m-vectors (lane i)
   int st_f64, st_flags;
   // mixed precision: hc[] keeps H in FP64 (the refinement's operator) and
-  // lf[] holds the FP32 factor (lane-owned column); its D^-1, Y, F live in
+  // lf2[] holds the FP32 factor (lane-owned column); its D^-1, Y, F live in
   // the FP64 factor's shared regions.
-  float lf[NP];
+  float2 lf2[NP / 2];  // (lf[2t], lf[2t + 1]): pairs for the packed FP32x2 updates
   int st_f32, st_sweeps;
   float dinvf, fdinvf;
   double pivot_max;
@@ -130,7 +130,6 @@ struct WarpQP {
       max_sweeps = prm.max_sweeps;
     }
   }
-
 
   // qv[i] = sym(Q)[i][lane]: (Q + Q')/2, or the coalesced Q[i][lane] alone
   // when Q is exactly symmetric (checked once per instance).  All loads are
@@ -389,26 +388,35 @@ struct WarpQP {
   }
 
   // Mixed: H (FP64 in hc, from form_hfull, kept there) rounded to FP32 and
-  // factored in FP32 in lf[]; Y = L^-1 A' in the same loop, F = Y' D^-1 Y
+  // factored in FP32 in lf2[]; Y = L^-1 A' in the same loop, F = Y' D^-1 Y
   // from the FP32 Y with FP64 products, and F's LDL^T, all in FP32.
   // Returns false when a pivot is not positive and finite or the pivot
   // ratio max(d)/min(d) of H exceeds pivot_max.
+  QPB_DEV float lfe(int k) const { return (k & 1) ? lf2[k >> 1].y : lf2[k >> 1].x; }
+
+  // The update of step k is S[i][j] += S[k][i] * (-S[k][j] / d_k): one FMA
+  // per element, two elements per packed FP32x2 FMA.  (Unlike the FP64
+  // factor, the row- and column-held copies of L may then differ by
+  // rounding: the FP32 factor only preconditions the FP64 refinement.)
   QPB_DEV bool ldlt32() {
 #pragma unroll
-    for (int i = 0; i < NP; ++i) lf[i] = __double2float_rn(hc[i]);
+    for (int t = 0; t < NP / 2; ++t) lf2[t] = make_float2(__double2float_rn(hc[2 * t]), __double2float_rn(hc[2 * t + 1]));
     int bad = 0;
     float dmax = 0.0f, dmin = INFINITY;
     float* cb = reinterpret_cast<float*>(a.cb());
-    float* yb = reinterpret_cast<float*>(a.Y());
-    float yc[MP];
+    float2* yb = reinterpret_cast<float2*>(a.Y());
+    float2 yc[MP / 2];
 #pragma unroll
-    for (int i = 0; i < MP; ++i) yc[i] = (lane < NP) ? __double2float_rn(a.A()[i * NP + lane]) : 0.0f;
+    for (int t = 0; t < MP / 2; ++t)
+      yc[t] = (lane < NP) ? make_float2(__double2float_rn(a.A()[2 * t * NP + lane]),
+                                        __double2float_rn(a.A()[(2 * t + 1) * NP + lane]))
+                          : make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      if (lane < NP) cb[lane] = lf[k];
+      if (lane < NP) cb[lane] = lfe(k);
       if (lane == k) {
 #pragma unroll
-        for (int i = 0; i < MP; ++i) yb[i] = yc[i];
+        for (int t = 0; t < MP / 2; ++t) yb[t] = yc[t];
       }
       __syncwarp();
       const float dk = cb[k];
@@ -419,18 +427,15 @@ struct WarpQP {
         dmin = fminf(dmin, dk);
       }
       if (lane == k) dinvf = rk;
-      const float hk = lf[k];
       if (lane > k) {
-        if ((k + 1) & 1) lf[k + 1] = fmaf(-(cb[k + 1] * hk), rk, lf[k + 1]);
+        const float nl = -(lfe(k) * rk);  // -L[lane][k]
+        const float2 nl2 = make_float2(nl, nl);
+        if ((k + 1) & 1) lf2[(k + 1) >> 1].y = fmaf(cb[k + 1], nl, lf2[(k + 1) >> 1].y);
 #pragma unroll
-        for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2) {
-          const float2 c2 = *reinterpret_cast<const float2*>(cb + i2);
-          lf[i2] = fmaf(-(c2.x * hk), rk, lf[i2]);
-          lf[i2 + 1] = fmaf(-(c2.y * hk), rk, lf[i2 + 1]);
-        }
-        const float l = hk * rk;
+        for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2)
+          lf2[i2 >> 1] = __ffma2_rn(*reinterpret_cast<const float2*>(cb + i2), nl2, lf2[i2 >> 1]);
 #pragma unroll
-        for (int i = 0; i < MP; ++i) yc[i] = fmaf(-l, yb[i], yc[i]);
+        for (int t = 0; t < MP / 2; ++t) yc[t] = __ffma2_rn(nl2, yb[t], yc[t]);
       }
       __syncwarp();
     }
@@ -439,7 +444,10 @@ struct WarpQP {
     if (lane < NP) {
       dvf[lane] = dinvf;
 #pragma unroll
-      for (int i = 0; i < MP; ++i) Yf[i * kYld + lane] = yc[i];
+      for (int t = 0; t < MP / 2; ++t) {
+        Yf[2 * t * kYld + lane] = yc[t].x;
+        Yf[(2 * t + 1) * kYld + lane] = yc[t].y;
+      }
     }
     __syncwarp();
     // F = Y' D^-1 Y: products of FP32 values are exact in FP64 (one DMMA
@@ -650,7 +658,7 @@ struct WarpQP {
 #pragma unroll
     for (int k = 0; k < NP - 1; ++k) {
       const float uk = __shfl_sync(kFull, u, k) * dvf[k];
-      if (lane > k) u = fmaf(-lf[k], uk, u);
+      if (lane > k) u = fmaf(-lfe(k), uk, u);
     }
     const float ud = (lane < NP) ? u * dinvf : 0.0f;
     float g = 0.0f;
@@ -679,7 +687,7 @@ struct WarpQP {
 #pragma unroll
     for (int k = NP - 1; k > 0; --k) {
       const float xk = __shfl_sync(kFull, xv, k);
-      if (lane < k) xv = fmaf(-lf[k] * dinvf, xk, xv);
+      if (lane < k) xv = fmaf(-lfe(k) * dinvf, xk, xv);
     }
     odx = (lane < n) ? xv : 0.0f;
   }
