@@ -427,16 +427,16 @@ struct WarpQP {
         dmin = fminf(dmin, dk);
       }
       if (lane == k) dinvf = rk;
-      if (lane > k) {
-        const float nl = -(lfe(k) * rk);  // -L[lane][k]
-        const float2 nl2 = make_float2(nl, nl);
-        if ((k + 1) & 1) lf2[(k + 1) >> 1].y = fmaf(cb[k + 1], nl, lf2[(k + 1) >> 1].y);
+      // branch-free: lanes <= k add c * 0 (their entries stay as they are;
+      // a non-finite pivot row fails the pivot checks anyway)
+      const float nl = (lane > k) ? -(lfe(k) * rk) : 0.0f;  // -L[lane][k]
+      const float2 nl2 = make_float2(nl, nl);
+      if ((k + 1) & 1) lf2[(k + 1) >> 1].y = fmaf(cb[k + 1], nl, lf2[(k + 1) >> 1].y);
 #pragma unroll
-        for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2)
-          lf2[i2 >> 1] = __ffma2_rn(*reinterpret_cast<const float2*>(cb + i2), nl2, lf2[i2 >> 1]);
+      for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2)
+        lf2[i2 >> 1] = __ffma2_rn(*reinterpret_cast<const float2*>(cb + i2), nl2, lf2[i2 >> 1]);
 #pragma unroll
-        for (int t = 0; t < MP / 2; ++t) yc[t] = __ffma2_rn(nl2, yb[t], yc[t]);
-      }
+      for (int t = 0; t < MP / 2; ++t) yc[t] = __ffma2_rn(nl2, yb[t], yc[t]);
       __syncwarp();
     }
     float* dvf = reinterpret_cast<float*>(a.dvi());
@@ -489,11 +489,9 @@ struct WarpQP {
         const float rk = __frcp_rn(dk);
         if (k < m) bad |= !(dk > 0.0f) || !isfinite(dk);
         if (lane == k) fdinvf = rk;
-        if (lane > k && lane < MP) {
-          const float f = fc[k] * rk;
+        const float f = (lane > k && lane < MP) ? -(fc[k] * rk) : 0.0f;  // branch-free, as above
 #pragma unroll
-          for (int i = k + 1; i < MP; ++i) fc[i] = fmaf(-cb[i], f, fc[i]);
-        }
+        for (int i = k + 1; i < MP; ++i) fc[i] = fmaf(cb[i], f, fc[i]);
         __syncwarp();
       }
       if (lane < MP) {
@@ -745,6 +743,16 @@ struct WarpQP {
           return true;
         }
         if (!(rel < 0.5 * prev)) return false;
+        if (sw > 1) {
+          // at the observed contraction c the last allowed sweep would stop
+          // only if rel * c^(max_sweeps - sw + 1) <= 1e-12: give up now
+          // otherwise (a stall restarts the iteration in FP64 from the same
+          // iterate, so the outcome is the same, without the futile sweeps)
+          const double c = rel / prev;
+          double pred = rel;
+          for (int j = sw; j <= max_sweeps; ++j) pred *= c;
+          if (pred > 1e-12) return false;
+        }
         prev = rel;
       }
     }
@@ -1004,7 +1012,9 @@ struct WarpQP {
     load(R, op == kOpSolve, from_iterate, src);
     double v1 = 0.0, v4 = 0.0, dxr = 0.0, dyr = 0.0;
     double sigma_mu = 0.0;
-    // bounded: initial point + 2 solves per iteration + adjoint
+    // bounded: initial point + 2 solves per iteration + adjoint; kept
+    // rolled (one copy of the stage code in the instruction cache)
+#pragma unroll 1
     for (int guard = 0; guard < 2 * kMaxIters + 4 && stage != kDone; ++guard) {
       // ---- prepare the system: weights, right-hand side, factor or not
       bool slack = true, refactor = true;
