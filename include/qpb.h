@@ -42,8 +42,15 @@ typedef enum {
 
 /* AUTO picks, per problem size, the fastest path that meets FP64 accuracy:
  * today the FP64 kernels (four instances per warp for n <= 8, m <= 2; one
- * warp per instance for n <= 32, m <= n_pad/4; one CTA per instance above).  MIXED forces FP32 factorisation with FP64
- * refinement; FP64 forces FP64 factorisation. */
+ * warp per instance for n <= 32, m <= n_pad/4; one CTA per instance above).
+ * MIXED factors in FP32 and refines every reduced KKT solve in FP64 (to
+ * 1e-12 of the solution) against the FP64 operator; an instance whose FP32
+ * factor has a pivot ratio max(d)/min(d) above pivot_max, or whose
+ * refinement stalls, continues with FP64 factors.  For n <= 32, m <= n_pad/4
+ * this is two launches on `stream`: the mixed one-warp kernel, then the
+ * FP64 one-warp kernel resuming the instances handed over to it (the
+ * workspace holds their iterates); above, one CTA per instance.  FP64 forces
+ * FP64 factorisation. */
 typedef enum { QPB_PRECISION_AUTO = 0, QPB_PRECISION_MIXED = 1, QPB_PRECISION_FP64 = 2 } qpb_precision;
 
 typedef enum {
@@ -72,7 +79,9 @@ typedef struct {
   int32_t team_threads; /* threads per instance: 0 = automatic, 32, 128 or 256
                            (128/256 force the one-CTA-per-instance kernel) */
   double pivot_max;     /* mixed: FP32 factor used while max(d)/min(d) <= pivot_max (0 = 1e7) */
-  int32_t max_sweeps;   /* mixed: FP64 refinement sweeps per solve before FP64 refactor (0 = 8) */
+  int32_t max_sweeps;   /* mixed: FP64 refinement sweeps per solve before FP64 refactor (0 = 8);
+                           refinement also gives up early when the observed contraction
+                           cannot reach 1e-12 within this many sweeps */
   int32_t* stats;       /* optional device int32[batch][4]: FP32 factorisations, FP64
                            factorisations, refinement sweeps, flag bits (1 FP32 factor
                            rejected, 2 refinement stalled, 4 FP64 pivot breakdown) */
@@ -262,9 +271,11 @@ int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const 
  * process exits.  Problems whose qpb_workspace_size exceeds 1 MiB are
  * rejected with QPB_ERR_UNSUPPORTED.  Problems planned with their instances
  * in shared memory need only 256 bytes of it, for any batch size: all
- * n <= 32 (FP64 and mixed), and mixed precision up to about n = 64 when
- * p = 2n; FP64 instances with n > 32 run from global arenas (more of them
- * stay resident per SM that way) and fit only in small batches.
+ * FP64 n <= 32, and mixed precision with n > 32 up to about n = 64 when
+ * p = 2n.  Mixed precision with n <= 32 also keeps a hand-over record per
+ * instance ((n + 2p + m) * 8 + 16 bytes: about 770 instances at n = 32,
+ * m = 8, p = 64); FP64 instances with n > 32 run from global arenas (more
+ * of them stay resident per SM that way) and fit only in small batches.
  * Nothing is allocated, by this call or by the library on its behalf.  The
  * first call on a device looks up the array's device address (one-time
  * set-up), so make that first call before any stream capture.  All calls
