@@ -111,11 +111,10 @@ struct WarpQP {
   double y, b;       // m-vectors (lane i)
   int st_f64, st_flags;
   // mixed precision: hc[] keeps H in FP64 (the refinement's operator) and
-  // lf2[] holds the FP32 factor (lane-owned column); its D^-1, Y, F live in
-  // the FP64 factor's shared regions.
+  // lf2[] holds column `lane` of the FP32 inverse of H; Y' = H^-1 A' and
+  // F^-1 live in the FP64 factor's shared regions.
   float2 lf2[NP / 2];  // (lf[2t], lf[2t + 1]): pairs for the packed FP32x2 updates
   int st_f32, st_sweeps;
-  float dinvf, fdinvf;
   double pivot_max;
   int max_sweeps;
 
@@ -362,7 +361,7 @@ struct WarpQP {
   QPB_DEV bool factor() {
     if constexpr (kMixed) {
       form_hfull();
-      if (ldlt32()) {
+      if (inv32()) {
         st_f32++;
         return true;
       }
@@ -388,81 +387,96 @@ struct WarpQP {
   }
 
   // Mixed: H (FP64 in hc, from form_hfull, kept there) rounded to FP32 and
-  // factored in FP32 in lf2[]; Y = L^-1 A' in the same loop, F = Y' D^-1 Y
-  // from the FP32 Y with FP64 products, and F's LDL^T, all in FP32.
-  // Returns false when a pivot is not positive and finite or the pivot
-  // ratio max(d)/min(d) of H exceeds pivot_max.
+  // inverted in FP32 in lf2[] (column `lane` of H^-1), then Y' = H^-1 A'
+  // (smem, FP32), F = A Y' (one FP64 tensor-core tile) and F^-1 (smem,
+  // FP32).  With explicit inverses every FP32 solve is a few independent
+  // dot products instead of two serial triangular sweeps.  Returns false
+  // when a pivot is not positive and finite or the pivot ratio
+  // max(d)/min(d) of H exceeds pivot_max.
   QPB_DEV float lfe(int k) const { return (k & 1) ? lf2[k >> 1].y : lf2[k >> 1].x; }
+  QPB_DEV void set_lfe(int k, float v) {
+    if (k & 1)
+      lf2[k >> 1].y = v;
+    else
+      lf2[k >> 1].x = v;
+  }
+  // Shared float regions of the inverse (inside the FP64 factor's regions):
+  // Y'[j][i] at Yf[i * kYld + j], float(A) at Af[i * NP + j] (during the
+  // factorisation only), F^-1 column-held at Ff[c * MP + i] = F^-1[i][c].
+  QPB_DEV float* Yf() const { return reinterpret_cast<float*>(a.Y()); }
+  QPB_DEV float* Af() const { return reinterpret_cast<float*>(a.Y()) + MP * kYld; }
+  QPB_DEV float* Ff() const { return reinterpret_cast<float*>(a.F()); }
 
-  // The update of step k is S[i][j] += S[k][i] * (-S[k][j] / d_k): one FMA
-  // per element, two elements per packed FP32x2 FMA.  (Unlike the FP64
-  // factor, the row- and column-held copies of L may then differ by
-  // rounding: the FP32 factor only preconditions the FP64 refinement.)
-  QPB_DEV bool ldlt32() {
+  // Symmetric sweep operator (Gauss-Jordan elimination of a symmetric
+  // positive definite matrix, in place): step k maps a_kk -> -1/a_kk,
+  // a_ik, a_kj -> a_ik / a_kk, a_kj / a_kk and a_ij -> a_ij - a_ik a_kj / a_kk;
+  // after all steps the matrix is -H^-1.  Its step-k pivot a_kk is the LDL^T
+  // pivot d_k.  Lane j holds column j; row k is column k (symmetry), so one
+  // broadcast per step serves every lane.  The step is branch-free: lane
+  // k's own column (its entries are the broadcast ones) is first scaled by
+  // 0 and then takes a_ik * (1/a_kk) from the same packed FMA.  (Folding it
+  // into one FMA with the multiplier 1/a_kk - 1 loses the relative accuracy
+  // of 1/a_kk for large pivots: measured 400x worse inverses.)
+  QPB_DEV bool inv32() {
 #pragma unroll
     for (int t = 0; t < NP / 2; ++t) lf2[t] = make_float2(__double2float_rn(hc[2 * t]), __double2float_rn(hc[2 * t + 1]));
     int bad = 0;
     float dmax = 0.0f, dmin = INFINITY;
     float* cb = reinterpret_cast<float*>(a.cb());
-    float2* yb = reinterpret_cast<float2*>(a.Y());
-    float2 yc[MP / 2];
-#pragma unroll
-    for (int t = 0; t < MP / 2; ++t)
-      yc[t] = (lane < NP) ? make_float2(__double2float_rn(a.A()[2 * t * NP + lane]),
-                                        __double2float_rn(a.A()[(2 * t + 1) * NP + lane]))
-                          : make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       if (lane < NP) cb[lane] = lfe(k);
-      if (lane == k) {
-#pragma unroll
-        for (int t = 0; t < MP / 2; ++t) yb[t] = yc[t];
-      }
       __syncwarp();
-      const float dk = cb[k];
-      const float rk = __frcp_rn(dk);
+      const float pk = cb[k];
+      const float rp = __frcp_rn(pk);
       if (k < n) {
-        bad |= !(dk > 0.0f) || !isfinite(dk);
-        dmax = fmaxf(dmax, dk);
-        dmin = fminf(dmin, dk);
+        bad |= !(pk > 0.0f) || !isfinite(pk);
+        dmax = fmaxf(dmax, pk);
+        dmin = fminf(dmin, pk);
       }
-      if (lane == k) dinvf = rk;
-      // branch-free: lanes <= k add c * 0 (their entries stay as they are;
-      // a non-finite pivot row fails the pivot checks anyway)
-      const float nl = (lane > k) ? -(lfe(k) * rk) : 0.0f;  // -L[lane][k]
-      const float2 nl2 = make_float2(nl, nl);
-      if ((k + 1) & 1) lf2[(k + 1) >> 1].y = fmaf(cb[k + 1], nl, lf2[(k + 1) >> 1].y);
+      const bool own = (lane == k);
+      const float akj = lfe(k);
+      const float c1 = own ? rp : -(akj * rp);
+      const float mu = own ? 0.0f : 1.0f;
+      const float2 c12 = make_float2(c1, c1), mu2 = make_float2(mu, mu);
 #pragma unroll
-      for (int i2 = ((k + 2) & ~1); i2 < NP; i2 += 2)
-        lf2[i2 >> 1] = __ffma2_rn(*reinterpret_cast<const float2*>(cb + i2), nl2, lf2[i2 >> 1]);
-#pragma unroll
-      for (int t = 0; t < MP / 2; ++t) yc[t] = __ffma2_rn(nl2, yb[t], yc[t]);
+      for (int t = 0; t < NP / 2; ++t)
+        lf2[t] = __ffma2_rn(*reinterpret_cast<const float2*>(cb + 2 * t), c12, __fmul2_rn(lf2[t], mu2));
+      set_lfe(k, own ? -rp : akj * rp);
       __syncwarp();
     }
-    float* dvf = reinterpret_cast<float*>(a.dvi());
-    float* Yf = reinterpret_cast<float*>(a.Y());
-    if (lane < NP) {
-      dvf[lane] = dinvf;
 #pragma unroll
-      for (int t = 0; t < MP / 2; ++t) {
-        Yf[2 * t * kYld + lane] = yc[t].x;
-        Yf[(2 * t + 1) * kYld + lane] = yc[t].y;
-      }
+    for (int t = 0; t < NP / 2; ++t) lf2[t] = make_float2(-lf2[t].x, -lf2[t].y);  // H^-1
+    // Y'[lane][i] = sum_l H^-1[lane][l] A[i][l] (column `lane` of H^-1 is row `lane`)
+    float* Yf = this->Yf();
+    float* Af = this->Af();
+    if (lane < NP) {
+#pragma unroll
+      for (int i = 0; i < MP; ++i) Af[i * NP + lane] = __double2float_rn(a.A()[i * NP + lane]);
     }
     __syncwarp();
-    // F = Y' D^-1 Y: products of FP32 values are exact in FP64 (one DMMA
-    // tile, as factor64), the sum rounded to FP32
-    float* Ff = reinterpret_cast<float*>(a.F());
+#pragma unroll
+    for (int i = 0; i < MP; ++i) {
+      float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int t = 0; t < NP / 2; ++t) acc = __ffma2_rn(lf2[t], *reinterpret_cast<const float2*>(Af + i * NP + 2 * t), acc);
+      if (lane < NP) Yf[i * kYld + lane] = acc.x + acc.y;
+    }
+    __syncwarp();
+    // F = A Y' (MP x MP, identity beyond m) on the FP64 tensor cores:
+    // F[g][c] = sum_k A[g][k] Y'[k][c], four k per step
+    float* Ff = this->Ff();
+    float fc[MP];
     {
       const int g = lane >> 2, t = lane & 3;
       double f0 = 0.0, f1 = 0.0;
 #pragma unroll
       for (int kb = 0; kb < NP / 4; ++kb) {
-        const int j = 4 * kb + t;
-        const double b0 = (g < MP) ? (double)Yf[g * kYld + j] : 0.0;
-        dmma884(f0, f1, b0 * (double)dvf[j], b0);
+        const int k = 4 * kb + t;
+        const double a0 = (g < MP) ? a.A()[g * NP + k] : 0.0;
+        const double b0 = (g < MP) ? (double)Yf[g * kYld + k] : 0.0;
+        dmma884(f0, f1, a0, b0);
       }
-      __syncwarp();
       if (g < MP) {
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
@@ -470,36 +484,35 @@ struct WarpQP {
           if (c < MP) Ff[g * MP + c] = (g < m && c < m) ? __double2float_rn(u ? f1 : f0) : (g == c ? 1.0f : 0.0f);
         }
       }
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < MP; ++i) fc[i] = (lane < MP) ? Ff[i * MP + lane] : 0.0f;  // column `lane` of F
+      __syncwarp();
+    }
+    // F^-1 by the same sweep, lanes 0..MP-1 (column-held), back to shared memory
+#pragma unroll
+    for (int k = 0; k < MP; ++k) {
+      if (lane == k) {
+#pragma unroll
+        for (int i = 0; i < MP; ++i) cb[i] = fc[i];
+      }
+      __syncwarp();
+      const float pk = cb[k];
+      const float rp = __frcp_rn(pk);
+      if (k < m) bad |= !(pk > 0.0f) || !isfinite(pk);
+      const bool own = (lane == k);
+      const float akc = fc[k];
+      const float c1 = own ? rp : -(akc * rp);
+#pragma unroll
+      for (int i = 0; i < MP; ++i) fc[i] = fmaf(cb[i], c1, own ? 0.0f : fc[i]);
+      fc[k] = own ? -rp : akc * rp;
+      __syncwarp();
+    }
+    if (lane < MP) {
+#pragma unroll
+      for (int i = 0; i < MP; ++i) Ff[lane * MP + i] = -fc[i];  // F^-1[i][lane]
     }
     __syncwarp();
-    fdinvf = 0.0f;
-    {
-      float fc[MP];
-#pragma unroll
-      for (int i = 0; i < MP; ++i) fc[i] = (lane < MP) ? Ff[i * MP + lane] : 0.0f;
-      __syncwarp();
-#pragma unroll
-      for (int k = 0; k < MP; ++k) {
-        if (lane == k) {
-#pragma unroll
-          for (int i = 0; i < MP; ++i) cb[i] = fc[i];
-        }
-        __syncwarp();
-        const float dk = cb[k];
-        const float rk = __frcp_rn(dk);
-        if (k < m) bad |= !(dk > 0.0f) || !isfinite(dk);
-        if (lane == k) fdinvf = rk;
-        const float f = (lane > k && lane < MP) ? -(fc[k] * rk) : 0.0f;  // branch-free, as above
-#pragma unroll
-        for (int i = k + 1; i < MP; ++i) fc[i] = fmaf(cb[i], f, fc[i]);
-        __syncwarp();
-      }
-      if (lane < MP) {
-#pragma unroll
-        for (int i = 0; i < MP; ++i) Ff[i * MP + lane] = fc[i];
-      }
-      __syncwarp();
-    }
     return !bad && (double)dmax <= pivot_max * (double)dmin;
   }
 
@@ -647,47 +660,50 @@ struct WarpQP {
     return v;
   }
 
-  // As reduced64, in FP32 with the FP32 factor.
+  // [H A'; A 0][dx; dy] = [r; v] in FP32 with the explicit inverses:
+  // t = H^-1 r, dy = F^-1 (Y'^T r - v), dx = t - Y' dy (F = A H^-1 A').
   QPB_DEV void reduced32(float r, float v, float& odx, float& ody) const {
-    const float* dvf = reinterpret_cast<const float*>(a.dvi());
-    const float* Yf = reinterpret_cast<const float*>(a.Y());
-    const float* Ff = reinterpret_cast<const float*>(a.F());
-    float u = (lane < n) ? r : 0.0f;
+    float* rb = reinterpret_cast<float*>(a.cb());
+    const float* Yf = this->Yf();
+    const float* Ff = this->Ff();
+    if (lane < NP) rb[lane] = (lane < n) ? r : 0.0f;
+    __syncwarp();
+    float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int k = 0; k < NP - 1; ++k) {
-      const float uk = __shfl_sync(kFull, u, k) * dvf[k];
-      if (lane > k) u = fmaf(-lfe(k), uk, u);
+    for (int t = 0; t < NP / 2; t += 2) {
+      a0 = __ffma2_rn(lf2[t], *reinterpret_cast<const float2*>(rb + 2 * t), a0);
+      if (t + 1 < NP / 2) a1 = __ffma2_rn(lf2[t + 1], *reinterpret_cast<const float2*>(rb + 2 * t + 2), a1);
     }
-    const float ud = (lane < NP) ? u * dinvf : 0.0f;
+    const float tj = (a0.x + a0.y) + (a1.x + a1.y);
+    // g_i = (Y'^T r)_i - v_i on lanes i < m (row i of the stored Y'^T)
     float g = 0.0f;
+    if (lane < MP) {
+      float g0 = 0.0f, g1 = 0.0f;
+#pragma unroll
+      for (int j = 0; j < NP; j += 2) {
+        g0 = fmaf(Yf[lane * kYld + j], rb[j], g0);
+        g1 = fmaf(Yf[lane * kYld + j + 1], rb[j + 1], g1);
+      }
+      g = (lane < m) ? (g0 + g1) - v : 0.0f;
+    }
+    // dy_i = sum_c F^-1[i][c] g_c on lanes i < m
+    float dy = 0.0f;
+#pragma unroll
+    for (int c = 0; c < MP; ++c) {
+      const float gc = __shfl_sync(kFull, g, c);
+      if (lane < MP) dy = fmaf(Ff[c * MP + lane], gc, dy);
+    }
+    dy = (lane < m) ? dy : 0.0f;
+    // dx_j = t_j - sum_i Y'[j][i] dy_i
+    float xv = tj;
 #pragma unroll
     for (int i = 0; i < MP; ++i) {
-      const float gi = wsumf((lane < NP ? Yf[i * kYld + lane] : 0.0f) * ud);
-      if (lane == i) g = gi - v;
+      const float di = __shfl_sync(kFull, dy, i);
+      if (lane < NP) xv = fmaf(-Yf[i * kYld + lane], di, xv);
     }
-    if (lane >= m) g = 0.0f;
-#pragma unroll
-    for (int k = 0; k < MP - 1; ++k) {
-      const float gk = __shfl_sync(kFull, g, k) * __shfl_sync(kFull, fdinvf, k);
-      if (lane > k && lane < MP) g = fmaf(-Ff[k * MP + lane], gk, g);
-    }
-    g = (lane < MP) ? g * fdinvf : 0.0f;
-#pragma unroll
-    for (int k = MP - 1; k > 0; --k) {
-      const float gk = __shfl_sync(kFull, g, k);
-      if (lane < k) g = fmaf(-Ff[k * MP + lane] * fdinvf, gk, g);
-    }
-    ody = (lane < m) ? g : 0.0f;
-    float wv = u;
-#pragma unroll
-    for (int i = 0; i < MP; ++i) wv = fmaf(-(lane < NP ? Yf[i * kYld + lane] : 0.0f), __shfl_sync(kFull, g, i), wv);
-    float xv = (lane < NP) ? wv * dinvf : 0.0f;
-#pragma unroll
-    for (int k = NP - 1; k > 0; --k) {
-      const float xk = __shfl_sync(kFull, xv, k);
-      if (lane < k) xv = fmaf(-lfe(k) * dinvf, xk, xv);
-    }
+    __syncwarp();  // rb read by every lane before the next broadcast
     odx = (lane < n) ? xv : 0.0f;
+    ody = dy;
   }
 
   // Mixed: FP32 solves with FP64 iterative refinement against the FP64
