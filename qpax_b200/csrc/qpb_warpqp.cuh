@@ -733,10 +733,27 @@ struct WarpQP {
         }
         double ad = 0.0, adx = 0.0;
 #pragma unroll
-        for (int i = 0; i < MP; ++i) {
-          ad = fma(ycol_a(i), __shfl_sync(kFull, dy, i), ad);
-          const double s = wsum(ycol_a(i) * dx);
-          if (lane == i) adx = s;
+        for (int i = 0; i < MP; ++i) ad = fma(ycol_a(i), __shfl_sync(kFull, dy, i), ad);
+        if constexpr (NP < 32) {  // (warp sums here: the row walk below spills at these budgets)
+#pragma unroll
+          for (int i = 0; i < MP; ++i) {
+            const double s = wsum(ycol_a(i) * dx);
+            if (lane == i) adx = s;
+          }
+        } else if (lane < MP) {
+          // (A dx)_lane from row `lane` of A and the broadcast dx; the
+          // rotated walk puts the MP lanes' 16-byte reads in distinct banks
+          const double* Ar = a.A() + lane * NP;
+          double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+          for (int t = 0; t < NP / 2; ++t) {
+            const int j = (2 * (t + lane)) & (NP - 1);
+            const double2 A2 = *reinterpret_cast<const double2*>(Ar + j);
+            const double2 x2 = *reinterpret_cast<const double2*>(xsv + j);
+            s0 = fma(A2.x, x2.x, s0);
+            s1 = fma(A2.y, x2.y, s1);
+          }
+          adx = s0 + s1;
         }
         rx = (lane < n) ? r - ((h0 + h1) + ad) : 0.0;
         ry = (lane < m) ? v - adx : 0.0;
