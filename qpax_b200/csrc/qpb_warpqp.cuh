@@ -394,12 +394,6 @@ struct WarpQP {
   // when a pivot is not positive and finite or the pivot ratio
   // max(d)/min(d) of H exceeds pivot_max.
   QPB_DEV float lfe(int k) const { return (k & 1) ? lf2[k >> 1].y : lf2[k >> 1].x; }
-  QPB_DEV void set_lfe(int k, float v) {
-    if (k & 1)
-      lf2[k >> 1].y = v;
-    else
-      lf2[k >> 1].x = v;
-  }
   // Shared float regions of the inverse (inside the FP64 factor's regions):
   // Y'[j][i] at Yf[i * kYld + j], float(A) at Af[i * NP + j] (during the
   // factorisation only), F^-1 column-held at Ff[c * MP + i] = F^-1[i][c].
@@ -423,27 +417,45 @@ struct WarpQP {
     int bad = 0;
     float dmax = 0.0f, dmin = INFINITY;
     float* cb = reinterpret_cast<float*>(a.cb());
+    const float2* cb2 = reinterpret_cast<const float2*>(cb);
+    // The step loop is rolled (one copy of two steps in the instruction
+    // cache): at the start of pass k (even) slot s of lf2[] holds entry
+    // (k + s) mod NP, so steps k and k + 1 find their pivot entry in slots 0
+    // and 1; each pass ends by rotating the slots by one pair.  After NP
+    // steps the slots are back in natural order.
+#pragma unroll 1
+    for (int k = 0; k < NP; k += 2) {
 #pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      if (lane < NP) cb[lane] = lfe(k);
-      __syncwarp();
-      const float pk = cb[k];
-      const float rp = __frcp_rn(pk);
-      if (k < n) {
-        bad |= !(pk > 0.0f) || !isfinite(pk);
-        dmax = fmaxf(dmax, pk);
-        dmin = fminf(dmin, pk);
+      for (int sg = 0; sg < 2; ++sg) {
+        const int kk = k + sg;
+        const float akj = sg ? lf2[0].y : lf2[0].x;  // this lane's entry kk
+        if (lane < NP) cb[lane] = akj;              // = column kk, natural order (symmetry)
+        __syncwarp();
+        const float pk = cb[kk];
+        const float rp = __frcp_rn(pk);
+        if (kk < n) {
+          bad |= !(pk > 0.0f) || !isfinite(pk);
+          dmax = fmaxf(dmax, pk);
+          dmin = fminf(dmin, pk);
+        }
+        const bool own = (lane == kk);
+        const float c1 = own ? rp : -(akj * rp);
+        const float mu = own ? 0.0f : 1.0f;
+        const float2 c12 = make_float2(c1, c1), mu2 = make_float2(mu, mu);
+#pragma unroll
+        for (int t = 0; t < NP / 2; ++t)  // slot pair t = entries k + 2t, k + 2t + 1
+          lf2[t] = __ffma2_rn(cb2[(k / 2 + t) & (NP / 2 - 1)], c12, __fmul2_rn(lf2[t], mu2));
+        const float nv = own ? -rp : akj * rp;
+        if (sg)
+          lf2[0].y = nv;
+        else
+          lf2[0].x = nv;
+        __syncwarp();
       }
-      const bool own = (lane == k);
-      const float akj = lfe(k);
-      const float c1 = own ? rp : -(akj * rp);
-      const float mu = own ? 0.0f : 1.0f;
-      const float2 c12 = make_float2(c1, c1), mu2 = make_float2(mu, mu);
+      const float2 first = lf2[0];
 #pragma unroll
-      for (int t = 0; t < NP / 2; ++t)
-        lf2[t] = __ffma2_rn(*reinterpret_cast<const float2*>(cb + 2 * t), c12, __fmul2_rn(lf2[t], mu2));
-      set_lfe(k, own ? -rp : akj * rp);
-      __syncwarp();
+      for (int t = 0; t < NP / 2 - 1; ++t) lf2[t] = lf2[t + 1];
+      lf2[NP / 2 - 1] = first;
     }
 #pragma unroll
     for (int t = 0; t < NP / 2; ++t) lf2[t] = make_float2(-lf2[t].x, -lf2[t].y);  // H^-1
@@ -455,7 +467,7 @@ struct WarpQP {
       for (int i = 0; i < MP; ++i) Af[i * NP + lane] = __double2float_rn(a.A()[i * NP + lane]);
     }
     __syncwarp();
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < MP; ++i) {
       float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
