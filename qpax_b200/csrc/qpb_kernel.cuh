@@ -63,7 +63,8 @@ KernelFn kernel_elastic_f64(int NT, int KC);
 KernelFn kernel_elastic_mixed(int NT, int KC);
 // One warp per instance, n <= NP (8, 16, 32), m <= NP / 4; FP64.
 KernelFn kernel_warp_f64(int NP);
-// As kernel_warp_f64 in mixed precision (FP32 factor, FP64 refinement).
+// As kernel_warp_f64 in mixed precision (FP32 inverses, FP64 refinement);
+// the instances it hands over are resumed by kernel_warp_f64 (resume launch).
 KernelFn kernel_warp_mixed(int NP);
 // 32 / NP instances per warp in lockstep (built for NP = 8); nullptr otherwise.
 KernelFn kernel_group_f64(int NP);

@@ -1,5 +1,7 @@
 // qpb_warpqp.cuh -- one warp per QP instance for n <= NP (NP = 8, 16, 32),
-// m <= MP = NP / 4, any p; FP64 throughout.
+// m <= MP = NP / 4, any p; FP64 (WarpQP<NP, MP>), or mixed precision
+// (WarpQP<NP, MP, true>: FP32 inverses with FP64 refinement, handing an
+// instance over to the FP64 kernel once its FP32 factor is rejected).
 //
 // Same method and formula order as qpb_std.cuh (qpax/pdip.py, pdip_relaxed.py,
 // diff_qp.py; citations there), laid out for a single warp so that no phase
