@@ -8,8 +8,9 @@ solver_tol 1e-6, target_kappa 1e-3, loss ||x - 1||^2:
   backward = qpb_solve_qp_primal_bwd (relaxation to kappa + adjoint KKT solve
              + the six gradient outer products)
 Inputs are resident in HBM; L2 is flushed (256 MB write) between steps,
-outside the per-step CUDA events.  Launch shapes are autotuned at setup
-(untimed).  Synthetic seeded data (no dataset).
+outside the per-step CUDA events.  Launch shapes of the default and mixed
+arms are autotuned at setup (untimed); the plain FP64 arm keeps its fixed
+one-CTA-per-QP shape.  Synthetic seeded data (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload dense|nnls|small|uneven|elastic] [--batch B]
@@ -569,7 +570,7 @@ def variants_for(spec: Spec, tune=True):
     v = {"auto": dict(precision="auto", tune=tune)}
     if spec.kind != "elastic":
         v["fp64_cta"] = dict(precision="fp64", team_threads=128)  # plain FP64, one QP per CTA
-    v["mixed"] = dict(precision="mixed")                          # FP32 factor + FP64 refinement
+    v["mixed"] = dict(precision="mixed", tune=tune)               # FP32 factor + FP64 refinement
     return v
 
 

@@ -311,15 +311,19 @@ int qpb_solve_qp_primal_bwd_packed(const qpb_plan* plan, const double* Q, const 
 
 extern "C" {
 
+// Tuning times one bin at a time from the start of the workspace (the
+// largest candidate of any bin), and afterwards every bin keeps its tuned
+// shape, laid out one after another: the bound is the sum over bins of each
+// bin's largest candidate (a tuned shape may need more than the heuristic's,
+// e.g. a global arena instead of shared memory).
 size_t qpb_plan_tune_workspace_size(const qpb_plan* plan) {
   if (!plan) return 0;
-  size_t need = plan->ws_bytes;
+  size_t total = 0;
   for (const PlanBin& b : plan->bins) {
     const qpb_dims d{b.count, b.n_max, b.m_max, b.p_max};
-    const size_t w = tune_workspace(kOpSolve, d, plan->cfg);
-    if (w > need) need = w;
+    total += (tune_workspace(kOpSolve, d, plan->cfg) + 255) & ~size_t(255);
   }
-  return need;
+  return total > plan->ws_bytes ? total : plan->ws_bytes;
 }
 
 int qpb_plan_tune(qpb_plan* plan, const double* Q, const double* q, const double* A, const double* b,

@@ -89,3 +89,30 @@ def test_elastic_tuning():
     assert fig["reference_only_converged_reproducible"] == 0, fig
     assert fig["iters_mismatch_both_converged_reproducible"] == 0, fig
     assert fig["gpu_only_max_kkt"] <= 1e-4 and fig["max_err_x"] <= 1e-6, fig
+
+
+def test_packed_plan_tuning_mixed():
+    """Mixed precision: tuning a plan whose bins run the mixed one-warp
+    kernel (n <= 32, two launches with hand-over records) and the mixed CTA
+    kernel (n > 32).  A tuned bin may need more workspace than its heuristic
+    shape; qpb_plan_tune_workspace_size covers every bin's largest
+    candidate.  The outputs meet the same bars as the FP64 plan's."""
+    from qpax_b200.packed import PackedPlan, pack, unpack
+
+    data = wl.uneven(256, seed=45, n_max=96)
+    shapes = [(len(q), len(b), len(h)) for q, b, h in zip(data[1], data[3], data[5])]
+    ins = [pack(v) for v in data]
+    plan = PackedPlan(shapes, precision="mixed")
+    x, s, z, y, conv, iters = plan.tune(*ins, 1e-6)
+    torch.cuda.synchronize()
+    L = plan.lengths
+    cut = lambda t, f: [v.cpu().numpy() for v in unpack(t, L[f])]
+    fig = parity.forward(data, 1e-6, dict(x=cut(x, 1), s=cut(s, 5), z=cut(z, 5), y=cut(y, 3),
+                                          conv=conv.cpu().numpy(), iters=iters.cpu().numpy()), eps=1e-12)
+    print(plan.bin_info(), fig)
+    assert fig["reference_only_converged_reproducible"] == 0, fig
+    assert fig["iters_mismatch_both_converged_reproducible"] == 0, fig
+    assert fig["gpu_only_max_kkt"] <= 1e-4 and fig["max_err_x"] <= 1e-6, fig
+    res2 = plan.solve(*ins, 1e-6)
+    for a, b_ in zip(res2, (x, s, z, y, conv, iters)):
+        assert torch.equal(a, b_)
