@@ -353,7 +353,6 @@ struct WarpQP {
   // Adds G' diag(w) G to hc (each element of the column exactly once).
   QPB_DEV void form_h_tensor() { form_h_onepass(); }
 
-
   // ---------------------------------------------------------------- factor
   // Factor for the weights in shared memory: FP64, or (mixed) FP32.
   // Returns false when the mixed kernel's FP32 factor is rejected: the
@@ -388,14 +387,6 @@ struct WarpQP {
     for (int i = 0; i < NP; ++i) hc[i] = (lane >= n && i == lane) ? 1.0 : qv[i] + hc[i];
   }
 
-  // Mixed: H (FP64 in hc, from form_hfull, kept there) rounded to FP32 and
-  // inverted in FP32 in lf2[] (column `lane` of H^-1), then Y' = H^-1 A'
-  // (smem, FP32), F = A Y' (one FP64 tensor-core tile) and F^-1 (smem,
-  // FP32).  With explicit inverses every FP32 solve is a few independent
-  // dot products instead of two serial triangular sweeps.  Returns false
-  // when a pivot is not positive and finite or the pivot ratio
-  // max(d)/min(d) of H exceeds pivot_max.
-  QPB_DEV float lfe(int k) const { return (k & 1) ? lf2[k >> 1].y : lf2[k >> 1].x; }
   // Shared float regions of the inverse (inside the FP64 factor's regions):
   // Y'[j][i] at Yf[i * kYld + j], float(A) at Af[i * NP + j] (during the
   // factorisation only), F^-1 column-held at Ff[c * MP + i] = F^-1[i][c].
@@ -403,6 +394,14 @@ struct WarpQP {
   QPB_DEV float* Af() const { return reinterpret_cast<float*>(a.Y()) + MP * kYld; }
   QPB_DEV float* Ff() const { return reinterpret_cast<float*>(a.F()); }
 
+  // Mixed: H (FP64 in hc, from form_hfull, kept there) rounded to FP32 and
+  // inverted in FP32 in lf2[] (column `lane` of H^-1), then Y' = H^-1 A'
+  // (smem, FP32), F = A Y' (one FP64 tensor-core tile) and F^-1 (smem,
+  // FP32).  With explicit inverses every FP32 solve is a few independent
+  // dot products instead of two serial triangular sweeps.  Returns false
+  // when a pivot is not positive and finite or the pivot ratio
+  // max(d)/min(d) of H exceeds pivot_max.
+  //
   // Symmetric sweep operator (Gauss-Jordan elimination of a symmetric
   // positive definite matrix, in place): step k maps a_kk -> -1/a_kk,
   // a_ik, a_kj -> a_ik / a_kk, a_kj / a_kk and a_ij -> a_ij - a_ik a_kj / a_kk;
