@@ -209,6 +209,10 @@ typedef struct qpb_plan_st qpb_plan;
 
 /* shapes: host int32[batch][3] = (n, m, p).  cfg as for the uniform calls. */
 int qpb_plan_create(qpb_plan** plan, int32_t batch, const int32_t* shapes, const qpb_config* cfg);
+/* Frees the plan's index tables, streams and events.  Calls already enqueued
+ * finish first (the tables are freed with cudaFree, which waits for the
+ * device), but a CUDA graph that captured a call with this plan reads those
+ * tables at every launch: destroy the plan only after its last launch. */
 int qpb_plan_destroy(qpb_plan* plan);
 /* Workspace bytes a call with this plan needs (every op). */
 size_t qpb_plan_workspace_size(const qpb_plan* plan);

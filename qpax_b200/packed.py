@@ -59,6 +59,17 @@ def sizes(shapes):
     return [n * n, n, m * n, m, p * n, p]
 
 
+def check_packed(t, length: int, dev: torch.device, name: str, dtype=torch.float64) -> None:
+    """Raise unless `t` is a contiguous `dtype` tensor of `length` elements on
+    `dev`: the kernels read and write exactly the plan's packed lengths, so a
+    shorter buffer would be read or written past its end on the device."""
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor, got {type(t).__name__}")
+    if t.dtype != dtype or t.device != dev or t.numel() != length or not t.is_contiguous():
+        what = f"{t.dtype} {tuple(t.shape)} on {t.device}" + ("" if t.is_contiguous() else ", not contiguous")
+        raise ValueError(f"{name}: expected a contiguous {dtype} tensor of {length} elements on {dev}, got {what}")
+
+
 def pack(arrays, device=None) -> torch.Tensor:
     """Concatenate per-instance arrays (any shapes) into one 1-D float64 tensor."""
     dev = device or _lib.device()
@@ -108,8 +119,13 @@ class PackedPlan:
     def new(self, k, dtype=torch.float64):
         return torch.empty(self.totals[k], dtype=dtype, device=self.dev)
 
+    def _check_inputs(self, tensors, fields, names):
+        for t, k, name in zip(tensors, fields, names):
+            check_packed(t, self.totals[k], self.dev, name)
+
     def solve(self, Q, q, A, b, G, h, solver_tol: float = 1e-3):
         """qpb_solve_qp_packed -> packed (x, s, z, y) and per-instance (converged, iters)."""
+        self._check_inputs((Q, q, A, b, G, h), range(6), "Q q A b G h".split())
         x, s, z, y = self.new(1), self.new(5), self.new(5), self.new(3)
         conv = torch.empty(self.batch, dtype=torch.int32, device=self.dev)
         iters = torch.empty(self.batch, dtype=torch.int32, device=self.dev)
@@ -124,6 +140,7 @@ class PackedPlan:
         size bin on this batch (forward solve on each bin's heaviest
         instances), keep the fastest per bin and record it for this device.
         Returns the packed solve outputs, like solve()."""
+        self._check_inputs((Q, q, A, b, G, h), range(6), "Q q A b G h".split())
         tw = int(self.lib.qpb_plan_tune_workspace_size(self.handle))
         ws = torch.empty(tw + 256, dtype=torch.uint8, device=self.dev)
         wp, wb = _lib.aligned(ws)
@@ -155,8 +172,13 @@ class PackedPlan:
 
         relax_out: optional (converged, iters) int32 device tensors of length
         batch that receive the relaxation's per-instance outcome."""
-        grads = [self.new(k) for k in range(6)]
+        self._check_inputs((Q, q, A, b, G, h, x, s, z, y, dl_dx), (0, 1, 2, 3, 4, 5, 1, 5, 5, 3, 1),
+                           "Q q A b G h x s z y dl_dx".split())
         rc, ri = relax_out if relax_out is not None else (None, None)
+        for t, name in ((rc, "relax_out[0]"), (ri, "relax_out[1]")):
+            if t is not None:
+                check_packed(t, self.batch, self.dev, name, torch.int32)
+        grads = [self.new(k) for k in range(6)]
         wp, wb = self._ws()
         _lib.call("qpb_solve_qp_primal_bwd_packed", self.handle,
                   *[_lib.ptr(t) for t in (Q, q, A, b, G, h, x, s, z, y, dl_dx)], ctypes.c_double(solver_tol),
