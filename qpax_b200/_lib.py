@@ -110,6 +110,15 @@ def as_f64(a, dev: torch.device) -> torch.Tensor:
     return t.contiguous()
 
 
+def rows(a, dev: torch.device, B: int, width: int, name: str) -> torch.Tensor:
+    """`a` as a contiguous float64 (B, width) tensor on `dev`, refusing any
+    other element count: the kernels read exactly B * width values of it."""
+    t = as_f64(a, dev)
+    if t.numel() != B * width:
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {B * width} values ({B} x {width})")
+    return t.reshape(B, width).contiguous()
+
+
 def ptr(t) -> int | None:
     if t is None:
         return None

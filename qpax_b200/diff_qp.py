@@ -12,6 +12,7 @@ Q, q, A, b, G, h -- the same custom_vjp qpax defines (:49-82).
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import torch
 
@@ -71,7 +72,8 @@ def diff_qp(Q, q, A, b, G, h, x, s, lam, nu, dl_dx, *, precision=None, team_thre
     """qpax/diff_qp.py:20 diff_qp at a given (relaxed) iterate -> (dQ, dq, dA, db, dG, dh)."""
     bt = StdBatch(Q, q, A, b, G, h)
     cfg = _config(dict(precision=precision, team_threads=team_threads))
-    its = [as_f64(t, bt.dev).reshape(bt.B, -1).contiguous() for t in (x, s, lam, nu, dl_dx)]
+    its = [_lib.rows(t, bt.dev, bt.B, w, nm) for t, w, nm in
+           zip((x, s, lam, nu, dl_dx), (bt.n, bt.p, bt.p, bt.m, bt.n), ("x", "s", "lam", "nu", "dl_dx"))]
     dQ, dq, dA = bt.new(bt.B, bt.n, bt.n), bt.new(bt.B, bt.n), bt.new(bt.B, bt.m, bt.n)
     db, dG, dh = bt.new(bt.B, bt.m), bt.new(bt.B, bt.p, bt.n), bt.new(bt.B, bt.p)
     _run("qpb_diff_qp", "diff", bt, cfg, [ptr(t) for t in its], [ptr(dQ), ptr(dq), ptr(dA), ptr(db), ptr(dG),
@@ -80,6 +82,46 @@ def diff_qp(Q, q, A, b, G, h, x, s, lam, nu, dl_dx, *, precision=None, team_thre
 
 
 _HOST_WS: dict = {}
+_HOST_LOCK = threading.Lock()
+
+
+def host_buffers(Q, q, A, b, G, h, dl_dx, out=None):
+    """Checked host tensors for the host-buffer pipeline.
+
+    Returns the seven inputs as contiguous CPU float64 tensors with a leading
+    batch axis, Q (B, n, n), q (B, n), A (B, m, n), b (B, m), G (B, p, n),
+    h (B, p), dl_dx (B, n), and the seven outputs x, dQ, dq, dA, db, dG, dh
+    (`out`, checked, or new tensors, pinned when a device is present).  The
+    pipeline copies exactly these sizes between host and device, so a buffer
+    of another size or layout is refused here rather than read or written
+    past its end."""
+    ins = [torch.as_tensor(t, dtype=torch.float64) for t in (Q, q, A, b, G, h, dl_dx)]
+    if any(t.device.type != "cpu" for t in ins):
+        raise ValueError("solve_qp_primal_vjp_host takes host (CPU) tensors")
+    Qh, _, Ah, _, Gh, _, _ = ins
+    if Qh.dim() != 3 or Ah.dim() != 3 or Gh.dim() != 3:
+        raise ValueError("solve_qp_primal_vjp_host takes batched inputs: Q (B, n, n), A (B, m, n), G (B, p, n)")
+    B, n, m, p = Qh.shape[0], Qh.shape[-1], Ah.shape[-2], Gh.shape[-2]
+    want = [(B, n, n), (B, n), (B, m, n), (B, m), (B, p, n), (B, p), (B, n)]
+    for name, t, w in zip(("Q", "q", "A", "b", "G", "h", "dl_dx"), ins, want):
+        if tuple(t.shape) != w:
+            raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {w}")
+    ins = [t.contiguous() for t in ins]
+    oshapes = [want[1], want[0], want[1], want[2], want[3], want[4], want[5]]
+    if out is None:
+        pin = torch.cuda.is_available()
+        out = [torch.empty(w, dtype=torch.float64, pin_memory=pin) for w in oshapes]
+    else:
+        out = list(out)
+        if len(out) != 7:
+            raise ValueError("out holds (x, dQ, dq, dA, db, dG, dh): 7 tensors")
+        for name, t, w in zip(("x", "dQ", "dq", "dA", "db", "dG", "dh"), out, oshapes):
+            if (not isinstance(t, torch.Tensor) or t.device.type != "cpu" or t.dtype != torch.float64
+                    or tuple(t.shape) != w or not t.is_contiguous()):
+                got = (f"{t.dtype} {tuple(t.shape)} on {t.device}" if isinstance(t, torch.Tensor)
+                       else type(t).__name__)
+                raise ValueError(f"out {name}: expected a contiguous CPU float64 tensor of shape {w}, got {got}")
+    return ins, out
 
 
 def _host_workspace(dev, nbytes):
@@ -105,15 +147,9 @@ def solve_qp_primal_vjp_host(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, 
     Returns (x, (dQ, dq, dA, db, dG, dh)) on the host; waits for completion.
     """
     dev = _lib.device()
-    ins = [torch.as_tensor(t, dtype=torch.float64) for t in (Q, q, A, b, G, h, dl_dx)]
-    if any(t.device.type != "cpu" for t in ins):
-        raise ValueError("solve_qp_primal_vjp_host takes host (CPU) tensors")
-    ins = [t.contiguous() for t in ins]
+    ins, out = host_buffers(Q, q, A, b, G, h, dl_dx, out)
     Qh, qh, Ah, bh, Gh, hh, gh = ins
     B, n, m, p = Qh.shape[0], Qh.shape[-1], Ah.shape[-2], Gh.shape[-2]
-    if out is None:
-        pin = torch.cuda.is_available()
-        out = [torch.empty(t.shape, dtype=torch.float64, pin_memory=pin) for t in (qh, Qh, qh, Ah, bh, Gh, hh)]
     dims = _lib.Dims(B, n, m, p)
     cfg = _config(dict(precision=precision, team_threads=team_threads))
     lib = _lib.load()
@@ -121,12 +157,15 @@ def solve_qp_primal_vjp_host(Q, q, A, b, G, h, dl_dx, solver_tol: float = 1e-5, 
     need = lib.qpb_solve_qp_primal_vjp_host_workspace_size(ctypes.byref(dims), chunks, ctypes.byref(cfg))
     if need == 0:
         raise _lib.QpbError(f"unsupported problem for the host pipeline: batch={B} n={n} m={m} p={p}")
-    wp, wb = _lib.aligned(_host_workspace(dev, need))
     stream = torch.cuda.current_stream(dev)
-    _lib.call("qpb_solve_qp_primal_vjp_host", ctypes.byref(dims), *[ptr(t) for t in ins],
-              ctypes.c_double(solver_tol), ctypes.c_double(target_kappa), *[ptr(t) for t in out], None, None,
-              chunks, ctypes.byref(cfg), wp, wb, stream.cuda_stream)
-    stream.synchronize()
+    # one cached workspace per device: calls from several threads take turns
+    # (each call waits for its own completion, so the turns are short-lived)
+    with _HOST_LOCK:
+        wp, wb = _lib.aligned(_host_workspace(dev, need))
+        _lib.call("qpb_solve_qp_primal_vjp_host", ctypes.byref(dims), *[ptr(t) for t in ins],
+                  ctypes.c_double(solver_tol), ctypes.c_double(target_kappa), *[ptr(t) for t in out], None, None,
+                  chunks, ctypes.byref(cfg), wp, wb, stream.cuda_stream)
+        stream.synchronize()
     return out[0], tuple(out[1:])
 
 

@@ -100,8 +100,10 @@ def initialize_elastic(Q, q, G, h, penalty, *, precision=None, team_threads=None
     return bt.out(*it)
 
 
-def _iter_in(bt, ts):
-    return [as_f64(t, bt.dev).reshape(bt.B, -1).contiguous() for t in ts]
+def _iter_in(bt, ts, names=("x", "t", "s1", "s2", "z1", "z2")):
+    """The elastic iterate (x (n), then t, s1, s2, z1, z2 (p each)) as checked (B, width) rows."""
+    widths = (bt.n,) + (bt.p,) * 5
+    return [_lib.rows(t, bt.dev, bt.B, w, nm) for t, w, nm in zip(ts, widths, names)]
 
 
 def relax_qp_elastic(Q, q, G, h, penalty, x, t, s1, s2, z1, z2, solver_tol: float = 1e-3,
@@ -123,7 +125,7 @@ def diff_qp_elastic(Q, q, G, h, x, t, s1, s2, lam1, lam2, dl_dx, *, penalty=0.0,
     """qpax/elastic_qp.py:381 diff_qp_elastic -> (dQ, dq, dG, dh)."""
     bt = ElasticBatch(Q, q, G, h, penalty)
     cfg = _config(dict(precision=precision, team_threads=team_threads))
-    ins = _iter_in(bt, (x, t, s1, s2, lam1, lam2))
+    ins = _iter_in(bt, (x, t, s1, s2, lam1, lam2), ("x", "t", "s1", "s2", "lam1", "lam2"))
     g = as_f64(dl_dx, bt.dev).reshape(bt.B, bt.n).contiguous()
     dQ, dq, dG, dh = bt.new(bt.B, bt.n, bt.n), bt.new(bt.B, bt.n), bt.new(bt.B, bt.p, bt.n), bt.new(bt.B, bt.p)
     _run("qpb_diff_qp_elastic", "elastic_diff", bt, cfg,

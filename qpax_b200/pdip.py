@@ -106,7 +106,7 @@ def relax_qp(Q, q, A, b, G, h, x, s, z, y, solver_tol: float = 1e-5, target_kapp
     """qpax/pdip_relaxed.py:70 relax_qp -> (xr, sr, zr, yr, converged, iters)."""
     bt = StdBatch(Q, q, A, b, G, h)
     cfg = _config(dict(precision=precision, team_threads=team_threads), stats)
-    its = [as_f64(t, bt.dev).reshape(bt.B, -1).contiguous() for t in (x, s, z, y)]
+    its = [_lib.rows(t, bt.dev, bt.B, w, nm) for t, w, nm in zip((x, s, z, y), (bt.n, bt.p, bt.p, bt.m), "xszy")]
     xr, sr, zr, yr = bt.new(bt.B, bt.n), bt.new(bt.B, bt.p), bt.new(bt.B, bt.p), bt.new(bt.B, bt.m)
     conv, iters = bt.new(bt.B, dtype=torch.int32), bt.new(bt.B, dtype=torch.int32)
     _run("qpb_relax_qp", "relax", bt, cfg,

@@ -189,29 +189,3 @@ def test_gpu_only_convergence_is_judged_by_its_kkt_residual(small_batch):
     fig, _ = parity.standard(data, TOL, KAPPA, dl, bad, ref=ref)
     assert fig["gpu_only_max_kkt"] > 0.1
 
-
-# --- host-side argument checks of the packed (uneven-batch) calls ------------
-
-
-def test_packed_arguments_are_checked_before_any_launch():
-    """PackedPlan passes raw pointers to kernels that touch exactly the plan's
-    packed lengths: a buffer of the wrong length, dtype, device or layout is
-    refused on the host."""
-    import torch
-
-    from qpax_b200.packed import check_packed
-
-    cpu = torch.device("cpu")
-    check_packed(torch.zeros(12, dtype=torch.float64), 12, cpu, "Q")
-    check_packed(torch.zeros(0, dtype=torch.float64), 0, cpu, "b")
-    check_packed(torch.zeros(5, dtype=torch.int32), 5, cpu, "conv", torch.int32)
-    with pytest.raises(ValueError, match="12 elements"):
-        check_packed(torch.zeros(11, dtype=torch.float64), 12, cpu, "Q")
-    with pytest.raises(ValueError, match="float64"):
-        check_packed(torch.zeros(12, dtype=torch.float32), 12, cpu, "Q")
-    with pytest.raises(ValueError, match="not contiguous"):
-        check_packed(torch.zeros(24, dtype=torch.float64)[::2], 12, cpu, "Q")
-    with pytest.raises(ValueError, match="on cuda"):
-        check_packed(torch.zeros(12, dtype=torch.float64), 12, torch.device("cuda", 0), "Q")
-    with pytest.raises(TypeError):
-        check_packed(np.zeros(12), 12, cpu, "Q")
