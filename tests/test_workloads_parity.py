@@ -7,7 +7,8 @@ the elastic batch).  oracle/parity.py computes the accuracy figures that the
 GPU tests and the benchmark report; here it is fed the oracle's own outputs
 (every figure must be zero) and copies of them with planted mistakes (each
 mistake must show in its figure).  Mistakes are planted in numpy copies of
-oracle outputs, on the CPU.
+oracle outputs, on the CPU.  oracle/conditioning.py, the analysis behind the
+default precision, is held to the pivot-ratio ranges it reports.
 """
 
 import numpy as np
@@ -189,3 +190,25 @@ def test_gpu_only_convergence_is_judged_by_its_kkt_residual(small_batch):
     fig, _ = parity.standard(data, TOL, KAPPA, dl, bad, ref=ref)
     assert fig["gpu_only_max_kkt"] > 0.1
 
+
+
+def test_reduced_kkt_conditioning_along_the_path():
+    """The measured basis of the precision choice: on the dense configuration
+    the reduced KKT matrix H = Q + G' diag(z/s) G is well conditioned early
+    in qpax's path and far beyond FP32 refinement (pivot ratio > 1e7, the
+    refactor rule) at the 1e-6 stopping point; at the relaxed point the
+    backward pass factors it is back within FP32 range."""
+    from oracle.conditioning import pivot_stats
+
+    Q, q, A, b, G, h = wl.config2(16)
+    _, s0, z0, _, _, _ = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=1e0)
+    r0, k0 = pivot_stats(Q, G, s0, z0)
+    x, s, z, y, conv, _ = oracle.solve_qp(Q, q, A, b, G, h, solver_tol=1e-6)
+    assert (conv == 1).all()
+    r6, k6 = pivot_stats(Q, G, s, z)
+    _, sr, zr, _, _, _ = oracle.relax_qp(Q, q, A, b, G, h, x, s, z, y, solver_tol=1e-6, target_kappa=1e-3)
+    rr, _ = pivot_stats(Q, G, sr, zr)
+    assert (r0 >= 1).all() and (r6 >= 1).all()
+    assert np.median(r0) < 1e5 and np.median(k0) * 2.0 ** -24 < 0.1
+    assert (r6 > 1e7).mean() >= 0.9 and np.median(k6) * 2.0 ** -24 > 1.0
+    assert np.median(rr) < 1e7
