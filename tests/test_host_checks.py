@@ -93,3 +93,23 @@ def test_iterates_are_checked_against_the_problem_widths():
         rows(np.zeros(16), CPU, 3, 4, "x")
     with pytest.raises(ValueError, match="s has shape"):
         rows(np.zeros((3, 5)), CPU, 3, 4, "s")
+
+
+def test_packed_layout_round_trip():
+    """The packed layout of an uneven batch: each array is the concatenation
+    of the per-instance row-major arrays in instance order; `sizes` gives
+    the per-instance lengths of Q, q, A, b, G, h and `unpack` inverts `pack`."""
+    from qpax_b200 import workloads as wl
+    from qpax_b200.packed import pack, sizes, unpack
+
+    data = wl.uneven(7, n_min=3, n_max=9, chunk=4)
+    shapes = [(len(q), len(b), len(h)) for q, b, h in zip(data[1], data[3], data[5])]
+    L = sizes(shapes)
+    for k, arrays in enumerate(data):
+        np.testing.assert_array_equal(L[k], [a.size for a in arrays])
+        t = pack(arrays, CPU)
+        assert t.dtype == torch.float64 and t.dim() == 1 and t.numel() == int(np.sum(L[k]))
+        parts = unpack(t, L[k], [a.shape for a in arrays])
+        for a, p in zip(arrays, parts):
+            np.testing.assert_array_equal(p.numpy(), a)
+    assert pack([], CPU).numel() == 0
